@@ -1,0 +1,164 @@
+"""Generate the golden fixtures in this folder from the reference itself.
+
+Runs the reference's numpy phasing path (dhparks/als_speckle, Python 2 source
+loaded unmodified through ``refshim``) on fixed, seeded inputs and stores
+inputs and outputs as ``.npz`` files.  Run it from the repository root in a
+container that has the reference checkout:
+
+    python tests/golden/make_golden.py [reference_root]
+
+The tests read only the ``.npz`` files; they never need the reference.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+if len(sys.argv) > 1:
+    os.environ["SPECKLE_REF_ROOT"] = sys.argv[1]
+import refshim  # noqa: E402
+
+ref = refshim.load_reference()
+
+
+def _quiet(fn, *a, **k):
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        return fn(*a, **k)
+
+
+def _inputs(N, seed):
+    rng = np.random.default_rng(seed)
+    # a smooth object in a centred box, its modulus, and a square support
+    B = max(2, N // 4)
+    obj = np.zeros((N, N), np.complex128)
+    c = N // 2
+    box = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.7, 0.7, (B, B)))
+    obj[c - B // 2:c - B // 2 + B, c - B // 2:c - B // 2 + B] = box
+    modulus = np.abs(np.fft.fft2(obj)).astype(np.float32)
+    support = np.zeros((N, N), np.float32)
+    S = min(N, B + max(2, N // 8))
+    support[c - S // 2:c - S // 2 + S, c - S // 2:c - S // 2 + S] = 1
+    psi = (rng.random((N, N)) + 1j * rng.random((N, N))).astype(np.complex64) * support
+    return psi.astype(np.complex64), modulus, support
+
+
+def projections():
+    """One reference iteration of each algorithm from a fixed state."""
+    out = {}
+    for N in (8, 32, 64):
+        psi, modulus, support = _inputs(N, 100 + N)
+        out["N%d_psi" % N] = psi
+        out["N%d_modulus" % N] = modulus
+        out["N%d_support" % N] = support
+        for alg in ("hio", "er", "raar", "sf", "dm"):
+            beta = 0.9 if alg != "raar" else 0.87
+            r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+            _quiet(r.load, modulus=modulus, support=support, numtrials=1)
+            r.psi_in = psi.copy()
+            _quiet(r.iterate, 1, order=((alg, 1),), beta=beta)
+            out["N%d_%s_psi_in" % (N, alg)] = np.asarray(r.psi_in)
+            out["N%d_%s_psi_out" % (N, alg)] = np.asarray(r.psi_out)
+            out["N%d_%s_beta" % (N, alg)] = np.float64(beta)
+            out["N%d_%s_savebuffer" % (N, alg)] = np.asarray(r.savebuffer)
+            out["N%d_%s_box" % (N, alg)] = np.array([r.r0, r.rows, r.c0, r.cols])
+    np.savez_compressed(os.path.join(HERE, "projections.npz"), **out)
+
+
+def trajectories():
+    """Short multi-iteration runs of the reference (default order, beta 0.8,
+    and a RAAR/DM schedule) from a seeded start."""
+    out = {}
+    N = 32
+    psi, modulus, support = _inputs(N, 7)
+    out["modulus"], out["support"], out["psi0"] = modulus, support, psi
+    for name, order, beta, iters in (("default", None, 0.8, 12),
+                                     ("hio_er", (("hio", 8), ("er", 2)), 0.9, 10),
+                                     ("raar_dm", (("raar", 3), ("dm", 2)), 0.87, 10)):
+        r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+        _quiet(r.load, modulus=modulus, support=support, numtrials=2)
+        r.psi_in = psi.copy()
+        _quiet(r.iterate, iters, order=order, beta=beta)
+        out[name + "_final"] = np.asarray(r.psi_in)
+        out[name + "_iters"] = np.int64(iters)
+        out[name + "_beta"] = np.float64(beta)
+    np.savez_compressed(os.path.join(HERE, "trajectories.npz"), **out)
+
+
+def seeds():
+    """``phasing.seed(val)`` output for a fixed val."""
+    N = 16
+    _, modulus, support = _inputs(N, 3)
+    r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+    _quiet(r.load, modulus=modulus, support=support, numtrials=1)
+    r.seed(1234)
+    np.savez_compressed(os.path.join(HERE, "seed.npz"), support=support,
+                        val=np.int64(1234), psi=np.asarray(r.psi_in))
+
+
+def helpers():
+    """bounding_box, refine_support, align_global_phase, prtf, align_frames,
+    center_of_mass_average on fixed inputs."""
+    out = {}
+    rng = np.random.default_rng(11)
+    # bounding boxes (including the test_mask.py known answer)
+    box = np.zeros((256, 256))
+    box[18:90, 45:63] = 1
+    cases = [(box, 0, False), (box, 14, False), (box, 10, False), (box, 4, True)]
+    blob = np.zeros((64, 64)); blob[3:20, 50:63] = 1
+    cases += [(blob, 10, False), (blob, 4, True), (blob, 0, True)]
+    for i, (d, pad, sq) in enumerate(cases):
+        out["bb%d_data" % i] = d.astype(np.float32)
+        out["bb%d_pad" % i] = np.int64(pad)
+        out["bb%d_square" % i] = np.int64(sq)
+        out["bb%d_box" % i] = ref.masking.bounding_box(d, pad=pad, force_to_square=sq)
+    # refine_support: two-part support, random magnitudes
+    N = 48
+    sup = np.zeros((N, N)); sup[6:20, 8:22] = 1; sup[28:44, 26:40] = 1
+    avg = (rng.random((N, N)) * sup + 0.05 * rng.random((N, N))) * np.exp(1j * rng.random((N, N)))
+    for j, (blur, lt, gt) in enumerate(((3, 0.2, 0.0), (1.5, 0.15, 0.05), (0.7, 0.3, 0.0))):
+        refined, blurred = _quiet(ref.phasing.refine_support, sup.copy(), avg, blur=blur,
+                                  local_threshold=lt, global_threshold=gt)
+        out["rs%d_support" % j] = sup
+        out["rs%d_avg" % j] = avg
+        out["rs%d_params" % j] = np.array([blur, lt, gt])
+        out["rs%d_refined" % j] = refined
+        out["rs%d_blurred" % j] = blurred
+    # align_global_phase on frames with random global phases
+    frames = (rng.random((5, 20, 24)) + 0.2j * rng.random((5, 20, 24)))
+    frames *= np.exp(1j * rng.uniform(0, 2 * np.pi, (5, 1, 1)))
+    frames = frames.astype(np.complex64)
+    out["agp_in"] = frames
+    out["agp_out"] = _quiet(ref.phasing.align_global_phase, frames)
+    # prtf
+    est = (rng.random((6, 12, 12)) * np.exp(1j * rng.normal(0, 0.3, (6, 12, 12)))).astype(np.complex64)
+    out["prtf_in"] = est
+    # prtf(N > rows) raises a broadcast error in the reference (phasing.py:1446-1448)
+    out["prtf_N12"] = _quiet(ref.phasing.prtf, est)
+    # align_frames (integer rolls), conditioning.py:316-430
+    data = rng.random((32, 32))
+    for k, (ry, rx) in enumerate(((3, 5), (0, 11), (15, 2))):
+        rolled = np.roll(np.roll(data, rx, axis=1), ry, axis=0)
+        out["af%d_rolled" % k] = rolled
+        out["af%d_coords" % k] = ref.conditioning.align_frames(rolled, data, return_type="coordinates")
+    out["af_ref"] = data
+    # center_of_mass_average
+    imgs = np.zeros((3, 24, 24), np.complex64)
+    for k, (dr, dc) in enumerate(((0, 0), (2, -3), (-4, 1))):
+        imgs[k, 8 + dr:14 + dr, 9 + dc:15 + dc] = (1 + k) * (1 + 0.5j)
+    out["com_in"] = imgs.copy()
+    out["com_out"] = ref.phasing.center_of_mass_average(imgs.copy())
+    np.savez_compressed(os.path.join(HERE, "helpers.npz"), **out)
+
+
+if __name__ == "__main__":
+    projections()
+    trajectories()
+    seeds()
+    helpers()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
