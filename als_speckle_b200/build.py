@@ -1,0 +1,103 @@
+"""Build libspeckle_b200.so for sm_100a from csrc/ with nvcc.
+
+Each .cu file is compiled to an object in ``_build/`` (in parallel, skipped
+when newer than every source and header), then all objects are linked into
+``libspeckle_b200.so`` next to this file, so the library travels with the
+source tree.
+
+    python -m als_speckle_b200.build [--force] [--jobs N]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libspeckle_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+         "--expt-relaxed-constexpr", "-I" + INCLUDE]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libspeckle_b200")
+
+
+def _cuda_home() -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+
+
+def _headers():
+    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+
+
+def _stale(obj: str, src: str, newest_header: float) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return t < os.path.getmtime(src) or t < newest_header
+
+
+def _compile(src: str, obj: str, verbose: bool) -> str:
+    cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
+    return r.stderr
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    newest = max([os.path.getmtime(h) for h in _headers()] + [os.path.getmtime(__file__)])
+    todo = []
+    objs = []
+    for src in sources:
+        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if force or _stale(obj, src, newest):
+            todo.append((src, obj))
+    if todo:
+        jobs = jobs or max(1, min(len(todo), os.cpu_count() or 1))
+        # largest units first so the pool finishes together
+        todo.sort(key=lambda so: -os.path.getsize(so[0]))
+        with cf.ThreadPoolExecutor(jobs) as ex:
+            futs = {ex.submit(_compile, s, o, verbose): s for s, o in todo}
+            for f in cf.as_completed(futs):
+                log = f.result()
+                if verbose and log:
+                    sys.stderr.write(log)
+    if todo or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+        tmp = LIB + ".tmp"
+        # the CUDA runtime is linked statically: the process may also hold
+        # torch's (older) libcudart, and the driver context is shared
+        cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + [
+            "-lcufft", "-Xlinker", "-rpath," + os.path.join(_cuda_home(), "lib64")]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(a.force, a.jobs, a.verbose))

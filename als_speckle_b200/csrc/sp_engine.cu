@@ -1,0 +1,362 @@
+// Host side of the fused iteration engine behind sp_engine_run (replaces
+// phasing.iterate, phasing.py:181-289, for many trials at once).
+//
+// Trials are split into groups whose working set (psi, G and, for DM, G2)
+// fits an L2 budget; each group runs its whole schedule before the next one
+// starts, so its planes stay resident in the 126 MB L2 across iterations.
+// Within a group, trials of the same size share one work list and each tick
+// launches one column-pass and one row-pass kernel per size present.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "sp_common.cuh"
+#include "sp_engine_launch.cuh"
+
+namespace sp {
+
+static cudaError_t launch_pass(int N, int E, int which, int grid, cudaStream_t st,
+                               const PassArgs& a) {
+  switch (N) {
+    case 8: return launch_pass_n8(E, which, grid, st, a);
+    case 16: return launch_pass_n16(E, which, grid, st, a);
+    case 32: return launch_pass_n32(E, which, grid, st, a);
+    case 64: return launch_pass_n64(E, which, grid, st, a);
+    case 128: return launch_pass_n128(E, which, grid, st, a);
+    case 256: return launch_pass_n256(E, which, grid, st, a);
+    case 512: return launch_pass_n512(E, which, grid, st, a);
+    case 1024: return launch_pass_n1024(E, which, grid, st, a);
+    case 2048: return launch_pass_n2048(E, which, grid, st, a);
+    case 4096: return launch_pass_n4096(E, which, grid, st, a);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static cudaError_t pass_setup(int N, int E, int* occ) {
+  switch (N) {
+    case 8: return pass_setup_n8(E, occ);
+    case 16: return pass_setup_n16(E, occ);
+    case 32: return pass_setup_n32(E, occ);
+    case 64: return pass_setup_n64(E, occ);
+    case 128: return pass_setup_n128(E, occ);
+    case 256: return pass_setup_n256(E, occ);
+    case 512: return pass_setup_n512(E, occ);
+    case 1024: return pass_setup_n1024(E, occ);
+    case 2048: return pass_setup_n2048(E, occ);
+    case 4096: return pass_setup_n4096(E, occ);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Per device, per (logN, E): dynamic-smem attribute set and occupancy cached.
+static std::mutex g_setup_mutex;
+static int g_occ[64][13][2];  // 0 = not yet configured
+static int g_sms[64];
+
+static cudaError_t occupancy_for(int N, int E, int* occ, int* sms) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  const int l = ilog2(N), k = (E >= 32 ? 1 : 0);
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (g_sms[dev] == 0) {
+    e = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+  }
+  if (g_occ[dev][l][k] == 0) {
+    int o = 0;
+    e = pass_setup(N, E, &o);
+    if (e != cudaSuccess) return e;
+    g_occ[dev][l][k] = std::max(1, o);
+  }
+  *occ = g_occ[dev][l][k];
+  *sms = g_sms[dev];
+  return cudaSuccess;
+}
+
+constexpr size_t kAlign = 256;
+static inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+static bool uses_dm(const sp_trial& t) {
+  for (int r = 0; r < t.n_runs; ++r)
+    if (t.run_alg[r] == SP_DM && t.run_count[r] > 0) return true;
+  return false;
+}
+
+static int default_e(int N) { return N >= 32 ? 32 : N; }
+
+static int chosen_e(int N, const sp_run_opts* opts) {
+  int E = default_e(N);
+  if (opts) {
+    const int l = ilog2(N);
+    if (opts->e_per_logn[l] > 0) E = opts->e_per_logn[l];
+  }
+  return effective_e(N, E);
+}
+
+static int validate(const sp_trial& t, int idx) {
+  SP_CHECK(is_pow2(t.n) && t.n >= kMinN && t.n <= kMaxN, SP_ERR_SIZE,
+           "trial %d: N=%d must be a power of two in [%d, %d]", idx, t.n, kMinN, kMaxN);
+  SP_CHECK(t.n_iter >= 0, SP_ERR_INVALID, "trial %d: n_iter < 0", idx);
+  SP_CHECK(t.n_runs >= 1 && t.n_runs <= SP_MAX_RUNS, SP_ERR_INVALID,
+           "trial %d: n_runs=%d not in [1, %d]", idx, t.n_runs, SP_MAX_RUNS);
+  int period = 0;
+  for (int r = 0; r < t.n_runs; ++r) {
+    SP_CHECK(t.run_alg[r] >= SP_HIO && t.run_alg[r] <= SP_SF_CPU, SP_ERR_INVALID,
+             "trial %d: unknown algorithm code %d", idx, t.run_alg[r]);
+    SP_CHECK(t.run_count[r] >= 0, SP_ERR_INVALID, "trial %d: negative run count", idx);
+    period += t.run_count[r];
+  }
+  SP_CHECK(period > 0, SP_ERR_INVALID, "trial %d: empty iteration order", idx);
+  SP_CHECK(t.psi_dev && t.modulus_dev && t.support_dev, SP_ERR_INVALID,
+           "trial %d: psi, modulus and support pointers are required", idx);
+  SP_CHECK(t.init == SP_INIT_GIVEN || t.init == SP_INIT_RANDOM_PHASE, SP_ERR_INVALID,
+           "trial %d: unknown init mode %d", idx, t.init);
+  if (uses_dm(t)) SP_CHECK(t.beta != 0.f, SP_ERR_INVALID, "trial %d: DM needs beta != 0", idx);
+  if (t.save_dev) {
+    SP_CHECK(t.r0 >= 0 && t.c0 >= 0 && t.rows > 0 && t.cols > 0 && t.r0 + t.rows <= t.n &&
+                 t.c0 + t.cols <= t.n,
+             SP_ERR_INVALID, "trial %d: crop box (%d,%d,%d,%d) outside %dx%d", idx, t.r0, t.c0,
+             t.rows, t.cols, t.n, t.n);
+  }
+  return SP_OK;
+}
+
+struct Layout {
+  size_t slots_off, items_off, planes_off, total;
+  std::vector<size_t> g_off, g2_off;
+  int n_items;
+};
+
+static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts) {
+  Layout L;
+  L.slots_off = 0;
+  L.items_off = align_up(sizeof(Slot) * (size_t)n);
+  // reserve item slots for the smallest E (most items), so the size does not
+  // depend on the radix choice
+  (void)opts;
+  int items = 0;
+  for (int i = 0; i < n; ++i) {
+    const int N = trials[i].n;
+    items += N / lines_per_item(N, effective_e(N, 16));
+  }
+  L.n_items = items;
+  L.planes_off = L.items_off + align_up(sizeof(Item) * (size_t)std::max(items, 1));
+  size_t off = L.planes_off;
+  L.g_off.resize(n);
+  L.g2_off.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const size_t plane = (size_t)trials[i].n * trials[i].n * sizeof(float2);
+    L.g_off[i] = off;
+    off += align_up(plane);
+    L.g2_off[i] = 0;
+    if (uses_dm(trials[i])) {
+      L.g2_off[i] = off;
+      off += align_up(plane);
+    }
+  }
+  L.total = off;
+  return L;
+}
+
+// one launch target: the items of one size within one group
+struct Segment {
+  int N, E, first, count, grid;
+};
+
+struct GraphKey {
+  void* ws;
+  int dev, group, n_ticks;
+  std::vector<int> shape;  // flattened segments
+  bool operator<(const GraphKey& o) const {
+    return std::tie(ws, dev, group, n_ticks, shape) <
+           std::tie(o.ws, o.dev, o.group, o.n_ticks, o.shape);
+  }
+};
+static std::mutex g_graph_mutex;
+static std::map<GraphKey, cudaGraphExec_t> g_graphs;
+static thread_local int64_t g_last_launches = 0;
+
+static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, const Item* items,
+                        int n_ticks, const float2* tw, cudaStream_t st) {
+  for (int k = 0; k < n_ticks; ++k) {
+    for (int which = 0; which < 2; ++which) {
+      for (const Segment& sg : segs) {
+        PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw};
+        SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid, st, a));
+      }
+    }
+  }
+  return SP_OK;
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+extern "C" int sp_engine_workspace_size(const sp_trial* trials, int n_trials, size_t* bytes) {
+  SP_CHECK(bytes != nullptr, SP_ERR_INVALID, "bytes is null");
+  SP_CHECK(n_trials >= 0 && (n_trials == 0 || trials), SP_ERR_INVALID, "no trials");
+  for (int i = 0; i < n_trials; ++i) {
+    SP_CHECK(is_pow2(trials[i].n) && trials[i].n >= kMinN && trials[i].n <= kMaxN, SP_ERR_SIZE,
+             "trial %d: N=%d must be a power of two in [%d, %d]", i, trials[i].n, kMinN, kMaxN);
+  }
+  *bytes = layout_for(trials, n_trials, nullptr).total;
+  return SP_OK;
+}
+
+extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspace_dev,
+                             size_t workspace_bytes, const sp_run_opts* opts, sp_stream_t stream) {
+  SP_CHECK(n_trials >= 0, SP_ERR_INVALID, "n_trials < 0");
+  if (n_trials == 0) return SP_OK;
+  SP_CHECK(trials != nullptr, SP_ERR_INVALID, "trials is null");
+  for (int i = 0; i < n_trials; ++i) {
+    const int st = validate(trials[i], i);
+    if (st != SP_OK) return st;
+  }
+  const Layout L = layout_for(trials, n_trials, opts);
+  SP_CHECK(workspace_dev != nullptr && workspace_bytes >= L.total, SP_ERR_WORKSPACE,
+           "workspace of %zu bytes given, %zu needed", workspace_bytes, L.total);
+  cudaStream_t st = as_stream(stream);
+  const float2* tw = nullptr;
+  SP_CUDA_TRY(twiddles(&tw));
+  char* ws = static_cast<char*>(workspace_dev);
+  int dev = 0;
+  SP_CUDA_TRY(cudaGetDevice(&dev));
+
+  // groups of consecutive trials whose working set fits the L2 budget
+  const int64_t budget = opts ? opts->l2_group_bytes : 0;
+  std::vector<int> gstart{0};
+  int64_t acc = 0;
+  for (int i = 0; i < n_trials; ++i) {
+    const int64_t plane = (int64_t)trials[i].n * trials[i].n * 8;
+    const int64_t need = plane * (uses_dm(trials[i]) ? 3 : 2);
+    if (budget > 0 && i > gstart.back() && acc + need > budget) {
+      gstart.push_back(i);
+      acc = 0;
+    }
+    acc += need;
+  }
+  gstart.push_back(n_trials);
+  const int n_groups = (int)gstart.size() - 1;
+
+  // slot descriptors and, per group and size, a contiguous run of items
+  std::vector<Slot> hs(n_trials);
+  std::vector<Item> hi;
+  hi.reserve(L.n_items);
+  std::vector<std::vector<Segment>> segs(n_groups);
+  std::vector<int> ticks(n_groups, 0);
+  for (int g = 0; g < n_groups; ++g) {
+    for (int N = kMinN; N <= kMaxN; N *= 2) {
+      const int E = chosen_e(N, opts);
+      const int L_items = N / lines_per_item(N, E);
+      const int first = (int)hi.size();
+      for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
+        if (trials[i].n != N) continue;
+        for (int b = 0; b < L_items; ++b) hi.push_back(Item{i, b});
+      }
+      const int count = (int)hi.size() - first;
+      if (count == 0) continue;
+      int occ = 1, sms = 1;
+      SP_CUDA_TRY(occupancy_for(N, E, &occ, &sms));
+      int per_sm = occ;
+      if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
+      segs[g].push_back(Segment{N, E, first, count, std::max(1, std::min(count, sms * per_sm))});
+    }
+    for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
+      const sp_trial& t = trials[i];
+      ticks[g] = std::max(ticks[g], t.n_iter + 1);
+      Slot& s = hs[i];
+      memset(&s, 0, sizeof(Slot));
+      s.logn = ilog2(t.n);
+      s.n_iter = t.n_iter;
+      s.n_runs = t.n_runs;
+      s.init = t.init;
+      int end = 0;
+      for (int r = 0; r < SP_MAX_RUNS; ++r) {
+        if (r < t.n_runs) {
+          end += t.run_count[r];
+          s.run_alg[r] = t.run_alg[r];
+        }
+        s.run_end[r] = end;
+      }
+      s.beta = t.beta;
+      s.seed = t.seed;
+      s.trial = t.trial;
+      s.r0 = t.r0;
+      s.c0 = t.c0;
+      s.rows = t.rows;
+      s.cols = t.cols;
+      s.start_tick = 0;
+      s.psi = static_cast<float2*>(t.psi_dev);
+      s.g = reinterpret_cast<float2*>(ws + L.g_off[i]);
+      s.g2 = L.g2_off[i] ? reinterpret_cast<float2*>(ws + L.g2_off[i]) : nullptr;
+      s.modulus = t.modulus_dev;
+      s.support = t.support_dev;
+      s.save = static_cast<float2*>(t.save_dev);
+      s.err = t.errors_dev;
+    }
+  }
+  SP_CUDA_TRY(cudaMemcpyAsync(ws + L.slots_off, hs.data(), sizeof(Slot) * hs.size(),
+                              cudaMemcpyHostToDevice, st));
+  if (!hi.empty())
+    SP_CUDA_TRY(cudaMemcpyAsync(ws + L.items_off, hi.data(), sizeof(Item) * hi.size(),
+                                cudaMemcpyHostToDevice, st));
+  for (int i = 0; i < n_trials; ++i) {
+    if (trials[i].errors_dev && trials[i].n_iter > 0)
+      SP_CUDA_TRY(cudaMemsetAsync(trials[i].errors_dev, 0,
+                                  sizeof(double) * 2 * (size_t)trials[i].n_iter, st));
+  }
+  const Slot* dslots = reinterpret_cast<const Slot*>(ws + L.slots_off);
+  const Item* ditems = reinterpret_cast<const Item*>(ws + L.items_off);
+  const bool use_graph = opts && opts->use_graph && st != nullptr;
+  g_last_launches = 0;
+  for (int g = 0; g < n_groups; ++g) g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
+
+  for (int g = 0; g < n_groups; ++g) {
+    if (!use_graph) {
+      const int rc = launch_ticks(segs[g], dslots, ditems, ticks[g], tw, st);
+      if (rc != SP_OK) return rc;
+      continue;
+    }
+    GraphKey key{workspace_dev, dev, g, ticks[g], {}};
+    for (const Segment& sg : segs[g]) key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid});
+    cudaGraphExec_t exec = nullptr;
+    {
+      std::lock_guard<std::mutex> lock(g_graph_mutex);
+      auto f = g_graphs.find(key);
+      if (f != g_graphs.end()) exec = f->second;
+    }
+    if (!exec) {
+      cudaGraph_t graph = nullptr;
+      SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int rc = launch_ticks(segs[g], dslots, ditems, ticks[g], tw, st);
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      if (rc != SP_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      SP_CUDA_TRY(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      SP_CUDA_TRY(ie);
+      std::lock_guard<std::mutex> lock(g_graph_mutex);
+      g_graphs[key] = exec;
+    }
+    SP_CUDA_TRY(cudaGraphLaunch(exec, st));
+  }
+  return SP_OK;
+}
+
+extern "C" int64_t sp_engine_last_launches(void) { return g_last_launches; }
+
+extern "C" int sp_engine_release_graphs(void) {
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  for (auto& kv : g_graphs) cudaGraphExecDestroy(kv.second);
+  g_graphs.clear();
+  return SP_OK;
+}

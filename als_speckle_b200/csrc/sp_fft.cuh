@@ -1,0 +1,215 @@
+// Stockham FFT building blocks for sm_100a.
+//
+// A line of N complex64 values (N a power of two, 2..4096) is transformed by
+// T = N/E threads that each hold E values in registers (E a power of two,
+// E <= N; 16 or 32 in the engine, chosen per N by the autotuner).  Thread t
+// always holds the elements with index t + i*T (i = 0..E-1): that is the input
+// read pattern of every Stockham stage and the output pattern of the last one,
+// so a forward transform, a pointwise operation and an inverse transform can be
+// chained in registers with no extra exchange.  Stage 1 is a radix-E DFT on the
+// registers; later stages (radix R <= E, E/R butterflies per thread) read from
+// and write to shared memory with the Stockham autosort index map
+//     out[(j/Ns)*Ns*R + (j%Ns) + r*Ns] = DFT_R( in[j + r*N/R] * W^(r*(j%Ns)) )
+// (Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC 2008).  Shared-memory addresses are padded with one
+// slot per 32 entries, which makes every exchange of the row and column layouts
+// below conflict-free for 8-byte accesses.
+//
+// Sign convention follows numpy: forward exp(-2*pi*i*n*k/N), inverse
+// exp(+2*pi*i*n*k/N), no scaling here (callers fold 1/N^2 into the projection).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sp {
+
+// ---------------------------------------------------------------------------
+// compile-time sin/cos (double precision Taylor series after octant reduction)
+// ---------------------------------------------------------------------------
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+__host__ __device__ constexpr double taylor_sin(double x) {
+  double term = x, sum = x, x2 = x * x;
+  for (int n = 1; n < 14; ++n) {
+    term *= -x2 / ((2.0 * n) * (2.0 * n + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr double taylor_cos(double x) {
+  double term = 1.0, sum = 1.0, x2 = x * x;
+  for (int n = 1; n < 14; ++n) {
+    term *= -x2 / ((2.0 * n - 1.0) * (2.0 * n));
+    sum += term;
+  }
+  return sum;
+}
+// cos(2*pi*k/R) and sin(2*pi*k/R) for integer k, R
+__host__ __device__ constexpr double cos_frac(int k, int R) {
+  k = ((k % R) + R) % R;
+  // reduce to first quadrant by symmetry
+  if (4 * k == R) return 0.0;
+  if (2 * k == R) return -1.0;
+  if (4 * k == 3 * R) return 0.0;
+  if (k == 0) return 1.0;
+  if (4 * k < R) return taylor_cos(2.0 * kPi * k / R);
+  if (2 * k < R) return -taylor_cos(2.0 * kPi * (R - 2 * k) / (2.0 * R));
+  if (4 * k < 3 * R) return -taylor_cos(2.0 * kPi * (2 * k - R) / (2.0 * R));
+  return taylor_cos(2.0 * kPi * (R - k) / R);
+}
+__host__ __device__ constexpr double sin_frac(int k, int R) {
+  return cos_frac(4 * k - R, 4 * R);  // sin(x) = cos(x - pi/2)
+}
+
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 w) {
+  return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+// a * conj(w)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 w) {
+  return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+// multiply by exp(DIR * 2*pi*i*K/R) with K, R compile-time constants
+template <int R, int DIR, int K>
+__device__ __forceinline__ float2 twiddle_const(float2 a) {
+  if constexpr (K == 0) {
+    return a;
+  } else if constexpr (4 * K == R) {
+    // DIR=-1: multiply by -i ; DIR=+1: multiply by +i
+    if constexpr (DIR < 0) return make_float2(a.y, -a.x);
+    else return make_float2(-a.y, a.x);
+  } else {
+    constexpr float c = (float)cos_frac(K, R);
+    constexpr float s = (float)(DIR * sin_frac(K, R));
+    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+  }
+}
+
+template <int R, int DIR, int K>
+__device__ __forceinline__ void dft_combine(float2* v, const float2* e, const float2* o) {
+  if constexpr (K < R / 2) {
+    const float2 t = twiddle_const<R, DIR, K>(o[K]);
+    v[K] = e[K] + t;
+    v[K + R / 2] = e[K] - t;
+    dft_combine<R, DIR, K + 1>(v, e, o);
+  }
+}
+
+// In-register DFT of size R (natural order in and out), radix-2 decimation in
+// time with compile-time twiddles; fully unrolled.
+template <int R, int DIR>
+__device__ __forceinline__ void dft(float2* v) {
+  if constexpr (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = a + b;
+    v[1] = a - b;
+  } else if constexpr (R > 2) {
+    float2 e[R / 2], o[R / 2];
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+      e[k] = v[2 * k];
+      o[k] = v[2 * k + 1];
+    }
+    dft<R / 2, DIR>(e);
+    dft<R / 2, DIR>(o);
+    dft_combine<R, DIR, 0>(v, e, o);
+  }
+}
+
+__host__ __device__ __forceinline__ constexpr int pad32(int a) { return a + (a >> 5); }
+
+// Shared-memory layouts for a Stockham index a in [0, N).
+// Rows: each line owns a contiguous padded strip.
+struct RowLayout {
+  float2* base;
+  __device__ __forceinline__ float2& at(int a) const { return base[pad32(a)]; }
+};
+// Column tiles: C lines interleaved element by element (line c is the column).
+struct ColLayout {
+  float2* base;
+  int C;
+  int c;
+  __device__ __forceinline__ float2& at(int a) const { return base[pad32(a) * C + c]; }
+};
+
+struct WarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct BlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// Stages 2.. of the Stockham transform.  NS = product of radices done so far.
+template <int N, int E, int DIR, int NS, class Lay, class Sync>
+__device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const Sync& sync,
+                                           bool active, int t, const float2* __restrict__ tw) {
+  constexpr int T = N / E;
+  if constexpr (NS < N) {
+    constexpr int R = (N / NS) < E ? (N / NS) : E;  // radix of this stage
+    constexpr int M = E / R;                        // butterflies per thread
+    constexpr bool LAST = (NS * R == N);
+    constexpr int TWS = N / (NS * R);               // table stride for W_{NS*R}
+    // read this stage's inputs: element t + i*T -> v[i]
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+    }
+    if constexpr (!LAST) sync();  // everyone has read before anyone overwrites
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int j = t + m * T;
+      const int k = j & (NS - 1);
+      float2 u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) u[r] = v[m + r * M];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = __ldg(&tw[(r * k) * TWS]);
+        u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
+      }
+      dft<R, DIR>(u);
+      if constexpr (LAST) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[m + r * M] = u[r];
+      } else {
+        const int base = (j / NS) * NS * R + k;
+        if (active) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) lay.at(base + r * NS) = u[r];
+        }
+      }
+    }
+    if constexpr (!LAST) {
+      sync();
+      fft_stages<N, E, DIR, NS * R, Lay, Sync>(v, lay, sync, active, t, tw);
+    }
+  }
+}
+
+// Full 1-D transform of one line held as v[i] = x[t + i*T]; on return
+// v[i] = X[t + i*T].  `tw` points at the N-entry table W_N^x = exp(-2 pi i x/N).
+// Every thread of the block must call this (it synchronises); inactive threads
+// pass active=false and skip all memory traffic.
+template <int N, int E, int DIR, class Lay, class Sync>
+__device__ __forceinline__ void fft_line(float2 (&v)[E], const Lay& lay, const Sync& sync,
+                                         bool active, int t, const float2* __restrict__ tw) {
+  static_assert(E <= N && (N % E) == 0, "E must divide N");
+  constexpr int T = N / E;
+  dft<E, DIR>(v);
+  if constexpr (T > 1) {
+    // stage-1 outputs go to out[t*E + r]
+    sync();  // previous readers of this shared buffer are done
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) lay.at(t * E + r) = v[r];
+    }
+    sync();
+    fft_stages<N, E, DIR, E, Lay, Sync>(v, lay, sync, active, t, tw);
+  }
+}
+
+}  // namespace sp

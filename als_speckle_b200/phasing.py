@@ -1,0 +1,457 @@
+"""Drop-in for ``speckle.phasing`` (dhparks/als_speckle, ``speckle/phasing.py``).
+
+Same class and function names, keyword arguments, defaults and state
+machine as the reference; the arithmetic runs in libspeckle_b200 on the GPU.
+Iterations are fused (one column pass and one row pass per iteration, see
+``csrc/sp_engine_kernels.cuh``); trials can also be run many at a time with
+``phasing.iterate_trials`` (an addition: the reference runs trials serially).
+
+Differences from the reference, all deliberate:
+* No CPU branch: ``force_cpu=True`` raises.  ER/SF follow the OpenCL kernels
+  (``phasing_er.cl``, ``phasing_sf.cl``); ``quirks="cpu"`` selects the
+  reference's CPU-branch forms instead (``phasing.py:1257``, ``:1284``).
+* Where ``|FFT(psi)| == 0`` the reference divides by zero
+  (``phasing_fourier.cl:14``); here the modulus is kept with zero phase.
+* Partial-coherence inputs (``ipsf``, ``spectrum``) and ``debug_on`` FITS
+  dumps are not supported and raise.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib, masking
+from ._lib import call, ptr, stream_ptr
+from .engine import Engine, TrialSpec, expand_runs
+from .gpu import common
+
+
+class phasing(common):
+    """A reconstruction: modulus, support, trials and a savebuffer
+    (``phasing.py:33-1353``)."""
+
+    def __init__(self, force_cpu=False, force_np_fft=False, gpu_info=None, device=None,
+                 quirks="gpu", engine=None):
+        if force_cpu:
+            raise ValueError("als_speckle_b200 has no CPU path; use the reference for force_cpu=True")
+        if not torch.cuda.is_available():
+            raise RuntimeError("als_speckle_b200 needs a CUDA device")
+        if quirks not in ("gpu", "cpu"):
+            raise ValueError("quirks must be 'gpu' or 'cpu'")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.use_gpu = True
+        self.compute_device = "gpu"
+        self.quirks = quirks
+        self.engine = engine or Engine(device=self.device, use_graph=False)
+        with torch.cuda.device(self.device):
+            call("sp_device_init")
+        self.modulus_state = 0
+        self.support_state = 0
+        self.ipsf_state = 0
+        self.buffer_state = 0
+        self.spectrum_state = 0
+        self.can_iterate = False
+        self.numtrial = 0
+        self.N = self.shape = self.size = None
+        self.modulus = self.support = self.psi_in = self.psi_out = None
+        self.numtrials = None
+        self.r0 = self.c0 = self.rows = self.cols = None
+        self.savebuffer = None
+        self.errors = None  # (iterations, 2) FP64 sums of the last iterate()
+        self.reconstruction = None
+
+    # ------------------------------------------------------------------ load
+    def load(self, modulus=None, support=None, ipsf=None, spectrum=None, numtrials=None):
+        """Load data (keyword arguments only), ``phasing.py:291-505``."""
+        for name, x in (("modulus", modulus), ("support", support), ("ipsf", ipsf)):
+            if x is not None and not isinstance(x, np.ndarray):
+                raise TypeError("%s must be ndarray if supplied" % name)
+        if ipsf is not None or spectrum is not None:
+            raise NotImplementedError("partial-coherence projections (ipsf, spectrum) are not supported")
+        if modulus is not None:
+            if modulus.ndim != 2:
+                raise ValueError("modulus must be 2d")
+            modulus = modulus.astype(np.float32)
+            if self.modulus_state == 2:
+                if modulus.shape != self.shape:
+                    raise ValueError("modulus shape %s differs from %s" % (modulus.shape, self.shape))
+            else:
+                if modulus.shape[0] != modulus.shape[1]:
+                    raise ValueError("modulus must be square")
+                N = modulus.shape[0]
+                if N & (N - 1) or not 8 <= N <= 4096:
+                    raise ValueError("N=%d must be a power of two in [8, 4096]" % N)
+                self.N, self.shape, self.size = N, modulus.shape, modulus.size
+                self.modulus = self._allocate(self.shape, np.float32, "modulus")
+                self.psi_in = self._allocate(self.shape, np.complex64, "psi_in")
+                self.psi_out = self._allocate(self.shape, np.complex64, "psi_out")
+            self.modulus = self._set(modulus, self.modulus)
+            self.modulus_state = 2
+        if support is not None:
+            if support.ndim != 2:
+                raise ValueError("support is %s-dim" % support.ndim)
+            if support.shape[0] != support.shape[1]:
+                raise ValueError("support shape is %s %s, must be square" % support.shape)
+            support = support.astype(np.float32)
+            support *= 1.0 / support.max()
+            if self.support_state == 2:
+                self.numtrial = 0
+            self._support_host = support
+            bounds = masking.bounding_box(support, pad=10)
+            self.r0, self.rows = int(bounds[0]), int(bounds[1] - bounds[0])
+            self.c0, self.cols = int(bounds[2]), int(bounds[3] - bounds[2])
+            self.support_state = 1
+        if numtrials is not None:
+            self.numtrials = int(numtrials)
+            if self.buffer_state == 0:
+                self.buffer_state = 1
+        if self.modulus_state == 2 and self.support_state > 0:
+            sup = self._support_host
+            if sup.shape != self.shape:
+                if self.rows > self.shape[0] or self.cols > self.shape[1]:
+                    raise ValueError("support crop larger than the modulus")
+                crop = sup[self.r0:self.r0 + self.rows, self.c0:self.c0 + self.cols]
+                new = np.zeros(self.shape, np.float32)
+                new[:self.rows, :self.cols] = crop
+                bounds = masking.bounding_box(new, force_to_square=True, pad=4)
+                self.r0, self.rows = int(bounds[0]), int(bounds[1] - bounds[0])
+                self.c0, self.cols = int(bounds[2]), int(bounds[3] - bounds[2])
+                sup = new
+                self._support_host = sup
+            self.support = self._allocate(self.shape, np.float32, "support")
+            self.support = self._set(sup, self.support)
+            self.support_state = 2
+            if self.buffer_state > 0:
+                shape = (self.numtrials + 1, self.rows, self.cols)
+                if self.buffer_state == 1 or tuple(self.savebuffer.shape) != shape:
+                    self.savebuffer = self._allocate(shape, np.complex64, "savebuffer")
+                    self.buffer_state = 2
+        self.can_iterate = self.modulus_state == 2 and self.support_state == 2 and self.buffer_state == 2
+
+    # ------------------------------------------------------------------ seed
+    def seed(self, val=None, supplied=None):
+        """psi_in = (U[0,1) + i U[0,1)) * support from numpy's global RNG, or a
+        supplied guess rolled onto the support (``phasing.py:990-1031``)."""
+        if self.N is None:
+            raise RuntimeError("cannot seed without N being set. load data first.")
+        if val is not None:
+            np.random.seed(val)
+        if supplied is None:
+            s = (np.random.rand(self.N, self.N) + 1j * np.random.rand(self.N, self.N)).astype(np.complex64)
+            s = s * self._support_host
+            self._set(s.astype(np.complex64), self.psi_in)
+            return
+        s = np.asarray(supplied)
+        if s.ndim != 2 or s.shape[0] > self.N or s.shape[1] > self.N:
+            raise ValueError("supplied guess must be 2d and no larger than N")
+        if s.shape != (self.N, self.N):
+            s2 = np.zeros(self.shape, np.complex64)
+            s2[:s.shape[0], :s.shape[1]] = s.astype(np.complex64)
+            s = s2
+        dev = torch.from_numpy(s.astype(np.complex64)).to(self.device)
+        ref = self.support.to(torch.complex64)
+        rolled = align_frames_device(dev, ref, use_mag_only=True)
+        rolled = rolled * self.support
+        self.psi_in.copy_(rolled)
+
+    # --------------------------------------------------------------- iterate
+    def _check_ready(self):
+        if not self.can_iterate:
+            raise RuntimeError("cant iterate before loading support, modulus and numtrials "
+                               "(states %d %d %d)" % (self.modulus_state, self.support_state,
+                                                      self.buffer_state))
+
+    def iterate(self, iterations, order=None, silent=True, beta=0.8, debug_on=None):
+        """Run ``iterations`` of the cyclic ``order`` on psi_in, then copy the
+        crop into ``savebuffer[numtrial]`` (``phasing.py:181-289``).
+
+        The per-iteration FP64 modulus error sums of FFT(psi_in) are kept in
+        ``self.errors`` (see ``modulus_error``)."""
+        if debug_on:
+            raise NotImplementedError("debug_on FITS dumps are not supported")
+        self._check_ready()
+        iterations = int(iterations)
+        if self.numtrial >= self.savebuffer.shape[0]:
+            raise IndexError("savebuffer is full (%d slots); load(numtrials=...) to enlarge"
+                             % self.savebuffer.shape[0])
+        algs, counts = expand_runs(order, self.quirks)
+        flat = [a for a, c in zip(algs, counts) for _ in range(c)]
+        chunk = iterations
+        if silent is not True:
+            chunk = 1 if isinstance(silent, bool) else max(1, int(silent))
+        self.errors = torch.zeros((iterations, 2), dtype=torch.float64, device=self.device)
+        done = 0
+        while done < iterations:
+            n = min(chunk, iterations - done)
+            rot = [flat[(done + i) % len(flat)] for i in range(len(flat))]
+            last = done + n >= iterations
+            spec = TrialSpec(psi=self.psi_in, modulus=self.modulus, support=self.support,
+                             iterations=n, order=_runs_from_flat(rot), beta=beta,
+                             box=(self.r0, self.c0, self.rows, self.cols) if last else None,
+                             save=self.savebuffer[self.numtrial] if last else None,
+                             errors=self.errors[done:done + n], quirks="gpu")
+            self.engine.solve([spec])
+            done += n
+            if silent is not True and (isinstance(silent, bool) or done % chunk == 0):
+                print("  iteration %s" % done)
+        if iterations == 0:
+            self._kexec("copy_to_buffer_f2", self.savebuffer, self.psi_in, self.c0, self.r0,
+                        self.numtrial, self.N, shape=(self.cols, self.rows))
+        self.numtrial += 1
+
+    def iterate_trials(self, iterations, trials, order=None, beta=0.8, seed=0,
+                       random_phase=True, errors=False):
+        """Batched extension: run ``trials`` independent starts at once and
+        fill ``savebuffer[numtrial:numtrial+trials]``.
+
+        Starts are S*IFFT(M exp(i phi)) with phi from (seed, trial index) when
+        ``random_phase``; otherwise every trial starts from the current psi_in.
+        Returns the final psi of every trial (trials, N, N) and, with
+        ``errors=True``, the FP64 error sums (trials, iterations, 2)."""
+        self._check_ready()
+        if self.numtrial + trials > self.savebuffer.shape[0]:
+            raise IndexError("savebuffer has %d free slots, %d trials requested"
+                             % (self.savebuffer.shape[0] - self.numtrial, trials))
+        psis = torch.empty((trials, self.N, self.N), dtype=torch.complex64, device=self.device)
+        if not random_phase:
+            psis.copy_(self.psi_in.expand(trials, self.N, self.N))
+        errs = (torch.zeros((trials, max(iterations, 1), 2), dtype=torch.float64, device=self.device)
+                if errors else None)
+        specs = []
+        for k in range(trials):
+            specs.append(TrialSpec(psi=psis[k], modulus=self.modulus, support=self.support,
+                                   iterations=int(iterations), order=order, beta=beta,
+                                   random_phase=random_phase, seed=seed, trial=self.numtrial + k,
+                                   box=(self.r0, self.c0, self.rows, self.cols),
+                                   save=self.savebuffer[self.numtrial + k],
+                                   errors=errs[k] if errors else None, quirks=self.quirks))
+        self.engine.solve(specs)
+        self.numtrial += trials
+        return (psis, errs) if errors else psis
+
+    def modulus_error(self):
+        """Per-iteration (E, R) of the last ``iterate``: E = sum(|F|-M)^2/sum M^2,
+        R = sum||F|-M|/sum M, F = FFT(psi_in) before each projection."""
+        m = self.modulus.double()
+        s2, s1 = float((m * m).sum()), float(m.sum())
+        e = self.errors.cpu().numpy()
+        return np.stack([e[:, 0] / s2, e[:, 1] / s1], axis=1)
+
+    def status(self):
+        ro = {2: "complete", 1: "incomplete", 0: "nothing"}
+        print("states:")
+        print("  modulus %s %s" % (ro[self.modulus_state], self.shape))
+        print("  support %s" % ro[self.support_state])
+        print("  ipsf    %s" % ro[self.ipsf_state])
+        print("  buffer  %s" % ro[self.buffer_state])
+        print("  spectrm %s" % ro[self.spectrum_state])
+        print("  device  %s" % self.compute_device)
+
+
+def _runs_from_flat(flat):
+    """Order list -> run-length ('alg', count) order with raw codes."""
+    runs = []
+    for a in flat:
+        if runs and runs[-1][0] == a:
+            runs[-1][1] += 1
+        else:
+            runs.append([a, 1])
+    return [(_CODE_NAMES[a], c) for a, c in runs]
+
+
+_CODE_NAMES = {_lib.SP_HIO: "hio", _lib.SP_ER: "er", _lib.SP_RAAR: "raar", _lib.SP_SF: "sf",
+               _lib.SP_DM: "dm", _lib.SP_ER_CPU: "er_cpu", _lib.SP_SF_CPU: "sf_cpu"}
+
+
+# ---------------------------------------------------------------------------
+# module functions
+# ---------------------------------------------------------------------------
+def _device_frames(data):
+    """(tensor on cuda complex64 (F, r, c), was_numpy, was_2d)."""
+    was_np = isinstance(data, np.ndarray)
+    t = torch.from_numpy(np.ascontiguousarray(data)).cuda() if was_np else data
+    if not torch.is_complex(t):
+        raise TypeError("data must be complex")
+    was2d = t.dim() == 2
+    if t.dim() not in (2, 3):
+        raise ValueError("data must be 2d or 3d")
+    t = t.to(torch.complex64)
+    if was2d:
+        t = t.unsqueeze(0)
+    return t.contiguous(), was_np, was2d
+
+
+def align_global_phase(data_in):
+    """Remove each frame's global phase: the minimiser of
+    sum|Re sin p + Im cos p|^2 from FP64 sums, then the sign rule
+    (``phasing.py:1355-1404``; closed form instead of ``fminbound``)."""
+    t, was_np, was2d = _device_frames(data_in)
+    t = t.clone()
+    F = t.shape[0]
+    sums = torch.empty(5 * F, dtype=torch.float64, device=t.device)
+    angles = torch.empty(F, dtype=torch.float64, device=t.device)
+    call("sp_align_global_phase", ptr(t), F, t[0].numel(), ptr(angles), ptr(sums), stream_ptr())
+    out = t[0] if was2d else t
+    return out.cpu().numpy() if was_np else out
+
+
+def prtf(estimates, N=None, silent=True, prtfq=False):
+    """|mean_n F_n/|F_n||, fftshifted, estimates embedded at the corner of
+    N x N (``phasing.py:1406-1461``, ``gpu_prtf`` ``:1463-1519``)."""
+    t, was_np, _ = _device_frames(estimates)
+    F, r, c = t.shape
+    if N is None:
+        N = max(r, c)
+    Np = 1 << (int(N) - 1).bit_length()
+    if Np != N:
+        raise ValueError("N=%d must be a power of two" % N)
+    work = torch.empty((F, N, N), dtype=torch.complex64, device=t.device)
+    out = torch.empty((N, N), dtype=torch.float32, device=t.device)
+    call("sp_prtf", ptr(t), F, r, c, N, ptr(work), ptr(out), stream_ptr())
+    res = out.cpu().numpy() if was_np else out
+    if prtfq:
+        arr = out.cpu().numpy()
+        return res, _annular_average(arr)
+    return res
+
+
+def gpu_prtf(gpuinfo, estimates, N=None, prtfq=False):
+    """``phasing.gpu_prtf`` signature; ``gpuinfo`` is ignored."""
+    return prtf(estimates, N=N, prtfq=prtfq)
+
+
+def _annular_average(arr):
+    """Average of ``arr`` over unit-width annuli about the centre (N/2, N/2),
+    radii 0..N/2-1: the ``prtfq`` output (reference: polar unwrap with
+    cubic interpolation then a row mean, ``phasing.py:1455-1458``)."""
+    N = arr.shape[0]
+    y, x = np.indices(arr.shape)
+    r = np.hypot(y - N // 2, x - N // 2)
+    ri = np.floor(r).astype(int)
+    keep = ri < N // 2
+    s = np.bincount(ri[keep], weights=arr[keep], minlength=N // 2)
+    n = np.bincount(ri[keep], minlength=N // 2)
+    return s / np.maximum(n, 1)
+
+
+def _gaussian_1d_kernel(n, sigma):
+    """fftshift of exp(-(x-n//2)^2/(2 sigma^2)), normalised: one factor of the
+    separable kernel of ``refine_support`` (``phasing.py:1787-1789`` with
+    ``shape.gaussian`` ``shape.py:494-508``)."""
+    x = np.arange(n).astype(float)
+    g = np.exp(-(x - n // 2) ** 2 / (2 * float(sigma) ** 2))
+    g = np.fft.fftshift(g)
+    return g / g.sum()
+
+
+def refine_support(support, average_mag, blur=3, local_threshold=.2, global_threshold=0,
+                   kill_weakest=False):
+    """Shrinkwrap (``phasing.py:1747-1815``): blur |avg| with a circular
+    Gaussian, keep the pixels above ``global_threshold`` of the maximum and,
+    within each connected part of ``support``, above ``local_threshold`` of
+    the part's maximum.  Returns (refined, blurred) as numpy arrays."""
+    support = np.asarray(support)
+    if support.ndim != 2:
+        raise ValueError("support must be 2d")
+    avg = average_mag
+    if isinstance(avg, np.ndarray):
+        if avg.ndim != 2:
+            raise ValueError("average_mag must be 2d")
+        avg_t = torch.from_numpy(np.ascontiguousarray(avg.astype(np.complex64))).cuda()
+    else:
+        avg_t = avg.to(torch.complex64).contiguous()
+    for name, v in (("blur", blur), ("global_threshold", global_threshold),
+                    ("local_threshold", local_threshold)):
+        if not isinstance(v, (float, int, np.floating, np.integer)):
+            raise TypeError("%s must be a number (is %s)" % (name, type(v)))
+    rows, cols = support.shape
+    if tuple(avg_t.shape) != (rows, cols):
+        raise ValueError("support and average_mag must have the same shape")
+    dev = avg_t.device
+    kr = torch.from_numpy(_gaussian_1d_kernel(rows, blur)).to(dev)
+    kc = torch.from_numpy(_gaussian_1d_kernel(cols, blur)).to(dev)
+    labels, n = masking.label_parts(support)
+    lab = torch.from_numpy(labels.astype(np.int32)).to(dev)
+    work = torch.empty(rows * cols + n + 1, dtype=torch.float64, device=dev)
+    blurred = torch.empty((rows, cols), dtype=torch.float64, device=dev)
+    refined = torch.empty((rows, cols), dtype=torch.float32, device=dev)
+    sums = torch.empty(n + 1, dtype=torch.float64, device=dev)
+    call("sp_shrinkwrap", ptr(avg_t), rows, cols, ptr(kr), ptr(kc), ptr(lab), n,
+         float(local_threshold), float(global_threshold), 1 if kill_weakest else 0,
+         ptr(work), ptr(blurred), ptr(refined), ptr(sums), stream_ptr())
+    ref = refined.cpu().numpy().astype(support.dtype if support.dtype.kind == "f" else np.int64)
+    return ref, blurred.cpu().numpy()
+
+
+def align_frames_device(frames, align_to, use_mag_only=False):
+    """Integer-roll alignment of N x N device frames to ``align_to``
+    (``conditioning.align_frames`` :316-430, ``crosscorr.alignment_coordinates``
+    :526-568).  Returns the rolled frames."""
+    single = frames.dim() == 2
+    fr = frames.unsqueeze(0) if single else frames
+    N = fr.shape[-1]
+    if fr.shape[-2] != N:
+        raise ValueError("frames must be square N x N")
+    ref = align_to.to(torch.complex64).contiguous()
+    work = torch.empty((2, N, N), dtype=torch.complex64, device=fr.device)
+    best = torch.empty(1, dtype=torch.int64, device=fr.device)
+    out = torch.empty_like(fr)
+    for k in range(fr.shape[0]):
+        f = fr[k].contiguous()
+        call("sp_xcorr_peak", ptr(f), ptr(ref), N, 1 if use_mag_only else 0, ptr(work), ptr(best),
+             stream_ptr())
+        key = int(best.item()) & 0xFFFFFFFFFFFFFFFF
+        sidx = 0xFFFFFFFF - (key & 0xFFFFFFFF)
+        mr, mc = divmod(sidx, N)
+        mr -= N // 2
+        mc -= N // 2
+        if mr > N // 2:
+            mr -= N
+        if mc > N // 2:
+            mc -= N
+        call("sp_roll", ptr(f), ptr(out[k]), N, N, -mr, -mc, stream_ptr())
+    return out[0] if single else out
+
+
+def center_of_mass_average(imgs):
+    """Sum of frames rolled so their |img| centres of mass coincide with the
+    first frame's (``phasing.py:1710-1745``)."""
+    t, was_np, _ = _device_frames(imgs)
+    F, r, c = t.shape
+    sums = torch.empty(3 * F, dtype=torch.float64, device=t.device)
+    call("sp_com_sums", ptr(t), F, r, c, ptr(sums), stream_ptr())
+    s = sums.cpu().numpy().reshape(F, 3)
+    coms = [(int(s[k, 1] / s[k, 0]), int(s[k, 2] / s[k, 0])) for k in range(F)]
+    shifts = np.array([(coms[k][0] - coms[0][0], coms[k][1] - coms[0][1]) for k in range(F)],
+                      np.int32)
+    sh = torch.from_numpy(shifts).to(t.device)
+    out = torch.empty((r, c), dtype=torch.complex64, device=t.device)
+    call("sp_roll_accumulate", ptr(t), F, r, c, ptr(sh), ptr(out), stream_ptr())
+    return out.cpu().numpy() if was_np else out
+
+
+def mean_frames(frames):
+    """Mean over the frame axis of device frames (complex64)."""
+    t, was_np, _ = _device_frames(frames)
+    out = torch.empty(t.shape[1:], dtype=torch.complex64, device=t.device)
+    call("sp_mean_frames", ptr(t), t.shape[0], t[0].numel(), ptr(out), stream_ptr())
+    return out.cpu().numpy() if was_np else out
+
+
+def fft2(x, inverse=False):
+    """Batched N x N complex FFT on the device (numpy conventions)."""
+    t = x.to(torch.complex64).contiguous()
+    N = t.shape[-1]
+    out = torch.empty_like(t)
+    call("sp_fft2", ptr(t), ptr(out), N, t.numel() // (N * N), 1 if inverse else 0, stream_ptr())
+    return out
+
+
+def rftf(*args, **kwargs):
+    raise NotImplementedError("rftf is not part of this engine yet")
+
+
+def covar_results(*args, **kwargs):
+    raise NotImplementedError("covar_results is not part of this engine yet")

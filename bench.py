@@ -1,0 +1,488 @@
+"""Benchmark: batched HIO phase retrieval, 512^2 x 128 trials (500 HIO + 50 ER).
+
+One step = one full reconstruction job: 128 seeded uniform-random-phase
+starts iterated 500 HIO (beta 0.9) + 50 ER through the fused engine, the crop
+saved per trial, then global-phase alignment, the average and the PRTF, all
+on the device.  The metric is trial-iterations per second over the job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own 128-trial job (weak scaling, no
+collective on the data path); the printed value is the sum over ranks
+divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 512
+TRIALS = 128
+ORDER = (("hio", 500), ("er", 50))
+ITERS = 550
+BETA = 0.9
+BYTES_PER_PX = 24  # algorithmic bytes per trial-iteration per pixel: psi r+w 16, modulus 4, support 4
+METRIC = "HIO trial-iterations/s, 512^2 x 128 trials (500 HIO + 50 ER), batched"
+UNIT = "trial-iter/s"
+WORKLOAD = "hio_512x128: N=512, 40 ellipses in a 128^2 box, 1e6 photons Poisson, support 160^2"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+        except Exception:
+            rows = []
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------- CPU side
+def _cpu_worker(args):
+    """One process: iterate the reference's numpy c64 algorithm (oracle port)."""
+    seed, iters = args
+    from als_speckle_b200 import synth  # noqa: F401  (pattern generation only)
+    from oracle import phasing_oracle as O
+    obj, M, S = synth.config_pattern("hio_512x128", seed=0)
+    psi = O.seed_random_phase(M, S, 1234, seed, mode="ref64")
+    t0 = time.perf_counter()
+    O.iterate(psi, M, S, iters, order=(("hio", iters),), beta=BETA, quirks="cpu", mode="ref64")
+    return time.perf_counter() - t0
+
+
+def cpu_run(procs, iters):
+    """Time `procs` independent trials x `iters` iterations on host cores."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        pool.map(_cpu_worker, [(k, iters) for k in range(procs)])
+    wall = time.perf_counter() - t0
+    return procs * iters / wall, wall
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(max_procs=64, iters=24):
+    procs = max(1, min(cpu_cores(), max_procs))
+    # warm the pool's imports once (not timed)
+    cpu_run(1, 1)
+    value, wall = cpu_run(procs, iters)
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+            "sample": "%d processes x 1 trial x %d HIO iterations at 512^2, reference numpy "
+                      "complex64 algorithm (oracle port), %.1f s wall" % (procs, iters, wall)}
+
+
+# ------------------------------------------------------------ GPU side
+def build_inputs(torch, device):
+    from als_speckle_b200 import synth
+    from als_speckle_b200.masking import bounding_box
+    obj, M, S = synth.config_pattern("hio_512x128", seed=0)
+    bb = bounding_box(S, pad=10)
+    box = (int(bb[0]), int(bb[2]), int(bb[1] - bb[0]), int(bb[3] - bb[2]))
+    return M, S, box
+
+
+class Job:
+    """Device-resident job: buffers allocated once, one step = full solve."""
+
+    def __init__(self, torch, device, M, S, box, engine, seed):
+        from als_speckle_b200.engine import TrialSpec
+        self.torch = torch
+        self.device = device
+        self.M = torch.from_numpy(M).to(device)
+        self.S = torch.from_numpy(S).to(device)
+        self.box = box
+        r0, c0, rows, cols = box
+        self.psis = torch.empty((TRIALS, N, N), dtype=torch.complex64, device=device)
+        self.save = torch.empty((TRIALS, rows, cols), dtype=torch.complex64, device=device)
+        self.errs = torch.zeros((TRIALS, ITERS, 2), dtype=torch.float64, device=device)
+        self.engine = engine
+        self.seed = seed
+        self.specs = [TrialSpec(psi=self.psis[k], modulus=self.M, support=self.S, iterations=ITERS,
+                                order=ORDER, beta=BETA, random_phase=True, seed=seed, trial=k,
+                                box=box, save=self.save[k], errors=self.errs[k])
+                      for k in range(TRIALS)]
+        self.prtf_work = torch.empty((TRIALS, N, N), dtype=torch.complex64, device=device)
+        self.prtf = torch.empty((N, N), dtype=torch.float32, device=device)
+        self.avg = torch.empty((rows, cols), dtype=torch.complex64, device=device)
+        self.sums = torch.empty(5 * TRIALS, dtype=torch.float64, device=device)
+        self.angles = torch.empty(TRIALS, dtype=torch.float64, device=device)
+        self.launches = 0
+
+    def step(self):
+        from als_speckle_b200._lib import call, ptr, stream_ptr, lib
+        self.engine.solve(self.specs)
+        eng = int(lib.sp_engine_last_launches())
+        r0, c0, rows, cols = self.box
+        s = stream_ptr()
+        call("sp_align_global_phase", ptr(self.save), TRIALS, rows * cols, ptr(self.angles),
+             ptr(self.sums), s)
+        call("sp_mean_frames", ptr(self.save), TRIALS, rows * cols, ptr(self.avg), s)
+        call("sp_prtf", ptr(self.save), TRIALS, rows, cols, N, ptr(self.prtf_work), ptr(self.prtf), s)
+        # align: 2 kernels, mean: 1, prtf: embed + 2 FFT passes + accumulate
+        self.launches = eng + 2 + 1 + 4
+
+    def r_factor(self):
+        m = self.M.double()
+        return (self.errs[:, -1, 1] / m.sum()).cpu().numpy()
+
+
+def flush_l2(torch, buf):
+    buf.fill_(1)
+
+
+def kernel_pass_times(torch, engine, job, reps=20):
+    """Average device time of one column-pass and one row-pass launch over
+    one L2 group, measured with CUDA events on the launching stream."""
+    from als_speckle_b200.engine import Engine
+    from als_speckle_b200 import _lib
+    group = max(1, int(engine.l2_group_bytes // (2 * N * N * 8))) if engine.l2_group_bytes else TRIALS
+    group = min(group, TRIALS)
+    eng = Engine(device=job.device, use_graph=False, l2_group_bytes=0, e_per_n=engine.e_per_n)
+    specs = job.specs[:group]
+    # one solve of 2 iterations gives launches C0 R0 C1 R1 C2 R2; time solves
+    # of 1 and 1+reps iterations and difference them to isolate steady ticks
+    import copy
+    def timed(iters):
+        sp = [copy.copy(s) for s in specs]
+        for s in sp:
+            s.iterations = iters
+            s.order = (("hio", iters),)
+            s.errors = None
+            s.save = None
+        eng.solve(sp)  # warm
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        eng.solve(sp)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3
+    t1 = timed(1)
+    tn = timed(1 + reps)
+    eng.close()
+    per_tick = (tn - t1) / reps
+    return per_tick, group
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    # a dedicated stream: CUDA graphs cannot be captured on the legacy default stream
+    torch.cuda.set_stream(torch.cuda.Stream(device))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+    from als_speckle_b200.engine import Engine
+    from als_speckle_b200 import autotune
+    tune = autotune.load_or_default(N)
+    engine = Engine(device=device, use_graph=True, l2_group_bytes=tune["l2_group_bytes"],
+                    e_per_n={N: tune["E"]})
+    M, S, box = build_inputs(torch, device)
+    job = Job(torch, device, M, S, box, engine, seed=1000 + rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # 256 MiB > L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        job.step()
+    barrier()
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_all0 = torch.cuda.Event(enable_timing=True)
+    t_all1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        t_all0.record(stream)
+        for k in range(args.steps):
+            flush_l2(torch, flush)
+            starts[k].record(stream)
+            job.step()
+            ends[k].record(stream)
+        t_all1.record(stream)
+        barrier()
+    total_s = t_all0.elapsed_time(t_all1) / 1e3
+    step_s = [s.elapsed_time(e) / 1e3 for s, e in zip(starts, ends)]
+    t = torch.tensor([total_s], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_s = float(t.item())
+    work = TRIALS * ITERS * world
+    value = work / total_s
+    launches = job.launches * args.steps
+    rfac = job.r_factor()
+
+    # e2e through the public API with host inputs and host outputs
+    e2e = run_e2e(torch, device, M, S, args, engine)
+    # kernel-level roofline: one steady iteration tick of one L2 group
+    per_tick, group = kernel_pass_times(torch, engine, job)
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_PX * N * N * group / per_tick / 1e9
+    plain = run_plain(torch, device, M, S)
+    single = run_single_trial(torch, device, M, S, engine)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (seeded ellipse objects, Poisson noise; reference example data unavailable)",
+        "config": {"workload": WORKLOAD, "trials": TRIALS, "iterations": "500 hio + 50 er",
+                   "beta": BETA, "l2": "inputs larger than L2 (512 MiB psi+G per job) and a "
+                   "256 MiB L2 flush before every step", "parallelism": "replicas x%d" % world,
+                   "E": tune["E"], "l2_group_bytes": tune["l2_group_bytes"]},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(step_s, 50)),
+                       "p99": 1e3 * float(np.percentile(step_s, 99))},
+        "final_r_factor": {"mean": float(np.mean(rfac)), "median": float(np.median(rfac))},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "kernel": "sp::col_pass_kernel<512,E> + sp::row_pass_kernel<512,E> "
+                               "(one iteration tick of %d trials, 24 B/px)" % group,
+                     "traffic": traffic_per_tick(group)},
+        "plain_gpu": plain,
+        "single_trial_engine": single,
+        "batched_over_plain": value / world / plain["value"],
+        "clocks": clk.summary(),
+    }
+    if args.cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line))
+
+
+def traffic_per_tick(group):
+    """DRAM bytes per tick from the committed ncu capture, scaled by trials."""
+    path = os.path.join(ROOT, "profiles", "traffic_hio_512.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        return float(t["dram_bytes_per_trial_tick"]) * group
+    except Exception:
+        return None
+
+
+def run_e2e(torch, device, M, S, args, engine):
+    """Same job through the phasing API with host buffers every step."""
+    from als_speckle_b200.phasing import phasing, align_global_phase, prtf, mean_frames
+    Mh = torch.from_numpy(M).pin_memory()
+    Sh = torch.from_numpy(S).pin_memory()
+    r = phasing(device=device, engine=engine)
+
+    def one():
+        r.numtrial = 0
+        r.load(modulus=Mh.numpy(), support=Sh.numpy(), numtrials=TRIALS)
+        psis, errs = r.iterate_trials(ITERS, TRIALS, order=ORDER, beta=BETA, seed=7, errors=True)
+        sb = r.savebuffer[:TRIALS]
+        al = align_global_phase(sb)
+        avg = mean_frames(al).cpu()
+        p = prtf(al, N=N).cpu()
+        rf = errs[:, -1, 1].cpu()
+        return avg.numel() * 8 + p.numel() * 4 + rf.numel() * 8
+
+    for _ in range(max(1, args.warmup)):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(args.steps):
+        d2h = one()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"value": TRIALS * ITERS * args.steps / dt, "unit": UNIT,
+            "h2d_bytes_per_step": int(M.nbytes + S.nbytes), "d2h_bytes_per_step": int(d2h),
+            "api": "phasing.load + iterate_trials + align_global_phase + mean_frames + prtf"}
+
+
+def run_plain(torch, device, M, S, iters=40):
+    """The plain single-instance path: one trial, cuFFT + one kernel per step
+    with a synchronisation after each (the reference's GPU dataflow)."""
+    from als_speckle_b200 import _lib
+    from als_speckle_b200.engine import expand_runs
+    Md = torch.from_numpy(M).to(device)
+    Sd = torch.from_numpy(S).to(device)
+    psi = torch.zeros((N, N), dtype=torch.complex64, device=device)
+    psi.real.copy_(Sd)
+    work = torch.empty((4, N, N), dtype=torch.complex64, device=device)
+    algs, counts = expand_runs((("hio", iters),))
+    a = (C.c_int32 * 1)(*algs)
+    c = (C.c_int32 * 1)(*counts)
+
+    def go(n):
+        _lib.call("sp_plain_iterate", N, n, 1, a, c, C.c_float(BETA), _lib.ptr(psi), _lib.ptr(Md),
+                  _lib.ptr(Sd), _lib.ptr(work), _lib.stream_ptr())
+    go(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    go(iters)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"value": iters / dt, "unit": "iter/s", "what": "1 trial, cuFFT + elementwise kernels, "
+            "sync after every launch (reference GPU dataflow)"}
+
+
+def run_single_trial(torch, device, M, S, engine, iters=200):
+    """The fused engine on a single trial (no batching)."""
+    from als_speckle_b200.engine import Engine, TrialSpec
+    Md = torch.from_numpy(M).to(device)
+    Sd = torch.from_numpy(S).to(device)
+    psi = torch.zeros((N, N), dtype=torch.complex64, device=device)
+    eng = Engine(device=device, use_graph=True, e_per_n=engine.e_per_n)
+    spec = TrialSpec(psi=psi, modulus=Md, support=Sd, iterations=iters, order=(("hio", iters),),
+                     beta=BETA, random_phase=True, seed=1)
+    eng.solve([spec])
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    eng.solve([spec])
+    b.record()
+    torch.cuda.synchronize()
+    eng.close()
+    return {"value": iters / (a.elapsed_time(b) / 1e3), "unit": "iter/s",
+            "what": "1 trial through the fused engine (CUDA graph)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = max(1, min(cpu_cores(), 64))
+    iters = 12
+    cpu_run(1, 1)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_run(procs, iters)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, _ = cpu_run(procs, iters)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    sample = ("%d processes x 1 trial x %d HIO iterations at 512^2 per step, the reference's "
+              "numpy complex64 algorithm (oracle port; the reference itself is Python 2 and "
+              "cannot run on the box)" % (procs, iters))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (seeded ellipse objects, Poisson noise)",
+        "config": {"workload": WORKLOAD, "trials": TRIALS, "iterations": "500 hio + 50 er",
+                   "beta": BETA},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
