@@ -102,6 +102,12 @@ def tune(N, trials=None, iters=60, path=CACHE, verbose=True):
 
 
 if __name__ == "__main__":
-    sizes = [int(a) for a in sys.argv[1:]] or [512]
-    for n in sizes:
-        print(n, tune(n))
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("sizes", type=int, nargs="*", default=[512])
+    ap.add_argument("--out", default=CACHE)
+    ap.add_argument("--trials", type=int, default=None)
+    ap.add_argument("--iters", type=int, default=60)
+    a = ap.parse_args()
+    for n in a.sizes:
+        print(n, tune(n, trials=a.trials, iters=a.iters, path=a.out))

@@ -295,7 +295,7 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_s = float(t.item())
-    work = TRIALS * ITERS * world
+    work = TRIALS * ITERS * world * args.steps
     value = work / total_s
     launches = job.launches * args.steps
     rfac = job.r_factor()
