@@ -1,0 +1,79 @@
+// sp_engine_run_static: the fused engine for callers that cannot allocate
+// device memory.
+//
+// sp_engine_run needs a scratch workspace (descriptor tables and one Fourier
+// work plane per trial) that the caller allocates.  Some callers cannot do
+// that: code running inside a host framework that owns every device
+// allocation and hands out only the buffers it created, plugins whose
+// allocator is not reachable from the thread that drives the GPU, or callers
+// that must not allocate after start-up for determinism.  For them this entry
+// point takes its scratch from a fixed array in device memory that belongs to
+// this library, and never allocates.
+//
+// The array is kStaticScratchBytes (48 MiB).  Every GPU that loads the library
+// holds it until the process exits.  Requests whose workspace would exceed it
+// are rejected with SP_ERR_SIZE before any work is enqueued.
+#include <cstring>
+#include <mutex>
+
+#include "sp_common.cuh"
+
+namespace sp {
+
+constexpr size_t kStaticScratchBytes = (size_t)48 << 20;
+
+// The scratch itself.  Host code must not use this name as an address: on the
+// host it is only a stand-in, so its device address is looked up once per
+// device with cudaGetSymbolAddress and that pointer is what gets passed on.
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mutex;
+static void* g_static_addr[256];
+
+// Device address of g_static_scratch on the current device (set up on the
+// first call for each device).
+static cudaError_t static_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (g_static_addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_addr[dev] = p;
+  }
+  *out = g_static_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+extern "C" int sp_engine_run_static(const sp_trial* trials, int n_trials, const sp_run_opts* opts,
+                                    sp_stream_t stream) {
+  SP_CHECK(n_trials >= 0, SP_ERR_INVALID, "n_trials < 0");
+  if (n_trials == 0) return SP_OK;
+  SP_CHECK(trials != nullptr, SP_ERR_INVALID, "trials is null");
+  size_t need = 0;
+  const int st = sp_engine_workspace_size(trials, n_trials, &need);
+  if (st != SP_OK) return st;
+  SP_CHECK(need <= kStaticScratchBytes, SP_ERR_SIZE,
+           "sp_engine_run_static: these trials need %zu bytes of scratch, more than the "
+           "%zu-byte static array; use sp_engine_run with a caller-allocated workspace",
+           need, kStaticScratchBytes);
+  void* scratch = nullptr;
+  SP_CUDA_TRY(static_scratch(&scratch));
+  // Eager launches only: the graphs cached by sp_engine_run are keyed by the
+  // workspace address and are not wanted for this shared array.
+  sp_run_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  o.use_graph = 0;
+  // Nothing in the scratch needs to start at zero: the descriptor tables are
+  // written by sp_engine_run on every call and each work plane is written
+  // before it is read.
+  return sp_engine_run(trials, n_trials, scratch, kStaticScratchBytes, &o, stream);
+}

@@ -110,6 +110,20 @@ int sp_engine_release_graphs(void);
  * (kernels inside a launched graph count individually). */
 int64_t sp_engine_last_launches(void);
 
+/* Same as sp_engine_run, but allocating nothing: for callers that cannot call
+ * cudaMalloc (a host framework that owns every device allocation, a plugin
+ * with no access to an allocator, or code that must not allocate once it is
+ * running).  No counterpart in the reference, which allocates its buffers in
+ * phasing.load.  Scratch comes from a 48 MiB array in device memory owned by
+ * this library, which every GPU that loads the library holds until exit;
+ * requests needing more (sp_engine_workspace_size) fail with SP_ERR_SIZE.
+ * The first call on each device looks up the array's address; make that first
+ * call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (other streams, other threads) race; nothing in it needs
+ * to start at zero.  Launches are eager (opts->use_graph is ignored). */
+int sp_engine_run_static(const sp_trial* trials, int n_trials, const sp_run_opts* opts,
+                         sp_stream_t stream);
+
 /* ---- operator API: one entry per reference OpenCL kernel --------------- */
 /* (gpu.py:295 _kexec name lookup; n = number of elements) */
 int sp_hio(float beta, const float* support_dev, const void* psi_in_dev, const void* psi_out_dev,
