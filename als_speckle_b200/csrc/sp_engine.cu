@@ -114,6 +114,8 @@ static int validate(const sp_trial& t, int idx) {
   SP_CHECK(period > 0, SP_ERR_INVALID, "trial %d: empty iteration order", idx);
   SP_CHECK(t.psi_dev && t.modulus_dev && t.support_dev, SP_ERR_INVALID,
            "trial %d: psi, modulus and support pointers are required", idx);
+  SP_CHECK(((uintptr_t)t.psi_dev | (uintptr_t)t.modulus_dev | (uintptr_t)t.support_dev) % 16 == 0,
+           SP_ERR_INVALID, "trial %d: psi, modulus and support must be 16-byte aligned", idx);
   SP_CHECK(t.init == SP_INIT_GIVEN || t.init == SP_INIT_RANDOM_PHASE, SP_ERR_INVALID,
            "trial %d: unknown init mode %d", idx, t.init);
   if (uses_dm(t)) SP_CHECK(t.beta != 0.f, SP_ERR_INVALID, "trial %d: DM needs beta != 0", idx);

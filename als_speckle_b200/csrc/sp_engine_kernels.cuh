@@ -63,72 +63,44 @@ __device__ __forceinline__ int slot_alg(const Slot& s, int i) {
 }
 
 // ---------------------------------------------------------------------------
-// real-space updates, same operation order as the OpenCL kernels
+// real-space updates
+//
+// Every update of the reference is linear in (psi_in, psi_out) with weights
+// that are affine in the support value s:
+//     new = pi * (a0 + a1 s) + po * (b0 + b1 s)        [ - s*beta*t for DM ]
+//   hio  phasing_hio.cl:16-17   (1-s)(pi - b po) + s po        a=(1,-1)  b=(-b, 1+b)
+//   er   phasing_er.cl:13-14    s po                           a=(0,0)   b=(0, 1)
+//   raar phasing_raar.cl:19-20  (1-s)(b pi + (1-2b) po) + s po a=(b,-b)  b=(1-2b, 2b)
+//   sf   phasing_sf.cl:16-17    (1-s)(-po) + s po              a=(0,0)   b=(-1, 2)
+//   er (CPU branch, phasing.py:1257)  s pi                     a=(0,1)   b=(0, 0)
+//   sf (CPU branch, phasing.py:1284)  (1-s)(-pi) + s po        a=(-1,1)  b=(0, 1)
+//   dm   phasing_dm2.cl:21-28 with g = -1/b:
+//        s(2po - b t + b((1+g)po - g pi)) + (1-s)(pi - b po)
+//        = pi + po(-b + (1+2b) s) - s b t                      a=(1,0)   b=(-b, 1+2b)
+// so one code path serves all of them.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 update_px(int alg, float b, float s, float2 pi, float2 po) {
-  float re, im;
+struct UpdateCoef {
+  float a0, a1, b0, b1;
+  bool needs_pi;
+};
+
+__device__ __forceinline__ UpdateCoef update_coef(int alg, float b) {
   switch (alg) {
-    case SP_HIO:  // phasing_hio.cl:16-17
-      re = (1 - s) * (pi.x - b * po.x) + s * po.x;
-      im = (1 - s) * (pi.y - b * po.y) + s * po.y;
-      break;
-    case SP_ER:  // phasing_er.cl:13-14
-      re = s * po.x;
-      im = s * po.y;
-      break;
-    case SP_RAAR: {  // phasing_raar.cl:12,19-20
-      const float b2 = 1 - 2 * b;
-      re = (1 - s) * (b * pi.x + b2 * po.x) + s * po.x;
-      im = (1 - s) * (b * pi.y + b2 * po.y) + s * po.y;
-      break;
-    }
-    case SP_SF:  // phasing_sf.cl:16-17
-      re = (1 - s) * (-1 * po.x) + s * po.x;
-      im = (1 - s) * (-1 * po.y) + s * po.y;
-      break;
-    case SP_ER_CPU:  // phasing.py:1257
-      re = s * pi.x;
-      im = s * pi.y;
-      break;
-    case SP_SF_CPU:  // phasing.py:1284
-      re = (1 - s) * (-1 * pi.x) + s * po.x;
-      im = (1 - s) * (-1 * pi.y) + s * po.y;
-      break;
-    default:
-      re = pi.x;
-      im = pi.y;
-      break;
-  }
-  return make_float2(re, im);
-}
-
-// psi_in <- update(psi_in, psi_out = v) for one line's E values
-template <int ALG, int E, int T>
-__device__ __forceinline__ void update_line(float2 (&v)[E], const Slot& s, size_t roff, float b) {
-  // ER and SF (kernel forms) do not read psi_in
-  constexpr bool kNeedsPsiIn = !(ALG == SP_ER || ALG == SP_SF);
-#pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const float sp = __ldg(&s.support[roff + i * T]);
-    const float2 pi = kNeedsPsiIn ? s.psi[roff + i * T] : make_float2(0.f, 0.f);
-    v[i] = update_px(ALG, b, sp, pi, v[i]);
+    case SP_HIO: return {1.f, -1.f, -b, 1.f + b, true};
+    case SP_ER: return {0.f, 0.f, 0.f, 1.f, false};
+    case SP_RAAR: return {b, -b, 1.f - 2.f * b, 2.f * b, true};
+    case SP_SF: return {0.f, 0.f, -1.f, 2.f, false};
+    case SP_ER_CPU: return {0.f, 1.f, 0.f, 0.f, true};
+    case SP_SF_CPU: return {-1.f, 1.f, 0.f, 1.f, true};
+    case SP_DM: return {1.f, 0.f, -b, 1.f + 2.f * b, true};
+    default: return {1.f, 0.f, 0.f, 0.f, true};
   }
 }
 
-// DM update without the -s*b*t term (phasing_dm2.cl:21-28, g = gamma_s = -1/b):
-//   s*(2po + b((1+g)po - g pi)) + (1-s)(pi - b po)
-__device__ __forceinline__ float2 dm_partial(float b, float s, float2 pi, float2 po) {
-  const float g = -1.0f / b;
-  const float t1r = 2 * po.x + b * ((1 + g) * po.x - g * pi.x);
-  const float t1i = 2 * po.y + b * ((1 + g) * po.y - g * pi.y);
-  const float t2r = pi.x - b * po.x;
-  const float t2i = pi.y - b * po.y;
-  return make_float2(s * t1r + (1 - s) * t2r, s * t1i + (1 - s) * t2i);
-}
-// dm1 (phasing_dm1.cl:16): -g (1-s) pi + s pi, g = gamma_m = 1/b
-__device__ __forceinline__ float2 dm1_px(float b, float s, float2 pi) {
+// dm1 (phasing_dm1.cl:16): -g (1-s) pi + s pi = pi (-g + (1+g) s), g = gamma_m = 1/b
+__device__ __forceinline__ float dm1_weight(float b, float s) {
   const float g = 1.0f / b;
-  return make_float2(-1 * g * (1 - s) * pi.x + s * pi.x, -1 * g * (1 - s) * pi.y + s * pi.y);
+  return -g + (1.f + g) * s;
 }
 
 __device__ __forceinline__ uint32_t hash_u32(uint32_t seed, uint32_t trial, uint32_t idx) {
@@ -142,16 +114,81 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t seed, uint32_t trial, uint
   return h;
 }
 
+// Streaming loads.  Pixel data is read once per pass, so it bypasses L1
+// (keeping L1 for nothing else is pointless: twiddles live in shared memory).
+// Read-only inputs (modulus, support) also take the non-coherent path.
+__device__ __forceinline__ float2 ld_stream(const float2* p) {
+  float2 v;
+  asm volatile("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_ro(const float* p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
+// Asynchronous global -> shared copies (cp.async, no registers held): psi,
+// support and modulus tiles are requested at the start of an item and land
+// while the item's first FFT runs.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copy `rows` rows of `row_bytes` (a multiple of 16) starting at gsrc with
+// global row pitch gpitch bytes into shared memory with row pitch spitch bytes.
+__device__ __forceinline__ void cp_async_rows(void* sdst, const void* gsrc, int rows, int row_bytes,
+                                              size_t gpitch, int spitch) {
+  const int per_row = row_bytes >> 4;
+  const int chunks = rows * per_row;
+  for (int q = threadIdx.x; q < chunks; q += blockDim.x) {
+    const int r = q / per_row, c = q - r * per_row;
+    cp_async<16>(static_cast<char*>(sdst) + r * spitch + (c << 4),
+                 static_cast<const char*>(gsrc) + r * gpitch + (c << 4));
+  }
+}
+
+// Shared-memory plan of one pass item.  Row pass: exchange strips | twiddles |
+// psi tile (L x N complex) | support tile (L rows of N + 16 floats).  Column
+// pass: exchange tile | twiddles | modulus tile (N rows x C floats).
+template <int N, int E>
+struct RowSmem {
+  static constexpr int L = lines_per_item(N, E);
+  static constexpr int kX = L * pad32(N);         // float2 entries
+  static constexpr int kTw = kX;                   // offset of the twiddle table
+  static constexpr int kPsi = kTw + N;
+  static constexpr int kSupPitch = N + 16;         // floats per support row
+  static constexpr int kSup = kPsi + L * N;        // offset (float2 units)
+  static constexpr int kTotal = kSup + (L * kSupPitch + 1) / 2;
+};
+template <int N, int E>
+struct ColSmem {
+  static constexpr int C = lines_per_item(N, E);
+  static constexpr int kX = C * pad32(N);
+  static constexpr int kTw = kX;
+  static constexpr int kMod = kTw + N;             // N rows x C floats
+  static constexpr int kTotal = kMod + (N * C + 1) / 2;
+};
+
 // ---------------------------------------------------------------------------
 // row pass for one item of a size-N slot
+//
+// The item's psi and support rows are requested with cp.async before the G
+// rows are loaded, so one memory latency is exposed per item and the update
+// reads them from shared memory.
 // ---------------------------------------------------------------------------
 template <int N, int E>
 __device__ __forceinline__ void row_item(const Slot& s, int step, int block, float2* smem,
-                                         const float2* __restrict__ tw_all) {
+                                         const float2* __restrict__ tw) {
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
   using Sync = typename std::conditional<(T <= 32), WarpSync, BlockSync>::type;
-  const float2* __restrict__ tw = tw_all + N;
   const int tid = threadIdx.x;
   const int lrow = tid / T;
   const int t = tid - lrow * T;
@@ -161,6 +198,8 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
   const Sync sync{};
   const float b = s.beta;
   const size_t roff = (size_t)row * N + t;
+  const float2* __restrict__ g_in = s.g + roff;
+  float2* psi = s.psi + roff;
 
   bool finish, start;
   int alg_f, alg_s;
@@ -176,46 +215,59 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
     alg_s = start ? slot_alg(s, step + 1) : SP_ER;
   }
 
+  using SM = RowSmem<N, E>;
+  // each thread only touches its own entries of the psi tile, so after the
+  // update has read psi_in the tile doubles as private storage for DM
+  float2* psi_s = smem + SM::kPsi + (active ? lrow : 0) * N + t;
+  const float* sup_s = reinterpret_cast<const float*>(smem + SM::kSup) +
+                       (active ? lrow : 0) * SM::kSupPitch + t;
   float2 v[E];
   if (finish) {
+    const UpdateCoef cf = update_coef(alg_f, b);
+    // psi (when the update reads it) and support rows -> shared memory
+    const size_t row0 = (size_t)block * L * N;
+    if (cf.needs_pi)
+      cp_async_rows(smem + SM::kPsi, s.psi + row0, 1, L * N * 8, 0, 0);
+    cp_async_rows(smem + SM::kSup, s.support + row0, L, N * 4, (size_t)N * 4, SM::kSupPitch * 4);
     if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = s.g[roff + i * T];
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(g_in + i * T);
     }
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out
+    cp_async_wait_all();
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const float sv = sup_s[i * T];
+        const float wa = cf.a0 + cf.a1 * sv;
+        const float wb = cf.b0 + cf.b1 * sv;
+        const float2 pi = cf.needs_pi ? psi_s[i * T] : make_float2(0.f, 0.f);
+        v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa + v[i].y * wb);
+      }
+    }
     if (alg_f == SP_DM) {
+      // v holds the update without -s*b*t (parked in the psi tile);
+      // t = IFFT_rows(G2) is the second projection
+      if (active) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) psi_s[i * T] = v[i];
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g2 + roff + i * T);
+      }
+      fft_line<N, E, +1>(v, lay, sync, active, t, tw);
       if (active) {
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-          const float sp = __ldg(&s.support[roff + i * T]);
-          s.psi[roff + i * T] = dm_partial(b, sp, s.psi[roff + i * T], v[i]);
+          const float w = sup_s[i * T] * b;
+          const float2 p = psi_s[i * T];
+          v[i] = make_float2(p.x - w * v[i].x, p.y - w * v[i].y);
         }
-#pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = s.g2[roff + i * T];
-      }
-      fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = second projection
-      if (active) {
-#pragma unroll
-        for (int i = 0; i < E; ++i) {
-          const float sp = __ldg(&s.support[roff + i * T]);
-          const float2 p = s.psi[roff + i * T];
-          v[i] = make_float2(p.x - sp * b * v[i].x, p.y - sp * b * v[i].y);
-        }
-      }
-    } else if (active) {
-      switch (alg_f) {
-        case SP_HIO: update_line<SP_HIO, E, T>(v, s, roff, b); break;
-        case SP_ER: update_line<SP_ER, E, T>(v, s, roff, b); break;
-        case SP_RAAR: update_line<SP_RAAR, E, T>(v, s, roff, b); break;
-        case SP_SF: update_line<SP_SF, E, T>(v, s, roff, b); break;
-        case SP_ER_CPU: update_line<SP_ER_CPU, E, T>(v, s, roff, b); break;
-        case SP_SF_CPU: update_line<SP_SF_CPU, E, T>(v, s, roff, b); break;
-        default: break;
       }
     }
     if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) s.psi[roff + i * T] = v[i];
+      for (int i = 0; i < E; ++i) psi[i * T] = v[i];
       if (!start && s.save != nullptr && row >= s.r0 && row < s.r0 + s.rows) {
         float2* dst = s.save + (size_t)(row - s.r0) * s.cols - s.c0;
 #pragma unroll
@@ -225,11 +277,29 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
         }
       }
     }
-  } else if (active) {
+  } else {
+    if (alg_s == SP_DM) {
+      cp_async_rows(smem + SM::kSup, s.support + (size_t)block * L * N, L, N * 4, (size_t)N * 4,
+                    SM::kSupPitch * 4);
+    }
+    if (active) {
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = s.psi[roff + i * T];
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(psi + i * T);
+    }
+    if (alg_s == SP_DM) {
+      cp_async_wait_all();
+      __syncthreads();
+    }
   }
   if (start) {
+    if (alg_s == SP_DM && active) {
+      // dm1(psi) waits in the psi tile while psi itself is transformed
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const float w = dm1_weight(b, sup_s[i * T]);
+        psi_s[i * T] = make_float2(v[i].x * w, v[i].y * w);
+      }
+    }
     fft_line<N, E, -1>(v, lay, sync, active, t, tw);
     if (active) {
 #pragma unroll
@@ -238,10 +308,7 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
     if (alg_s == SP_DM) {
       if (active) {
 #pragma unroll
-        for (int i = 0; i < E; ++i) {
-          const float sp = __ldg(&s.support[roff + i * T]);
-          v[i] = dm1_px(b, sp, s.psi[roff + i * T]);
-        }
+        for (int i = 0; i < E; ++i) v[i] = psi_s[i * T];
       }
       fft_line<N, E, -1>(v, lay, sync, active, t, tw);
       if (active) {
@@ -256,43 +323,39 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
 // column pass for one item of a size-N slot
 // ---------------------------------------------------------------------------
 template <int N, int E>
-__device__ __forceinline__ void project_cols(float2 (&v)[E], const float* __restrict__ mod,
-                                             size_t coff, bool active, double& e2, double& e1,
-                                             bool want_err) {
-  constexpr int T = N / E;
+__device__ __forceinline__ void project_cols(float2 (&v)[E], const float (&m)[E], bool active,
+                                             double& e2, double& e1, bool want_err) {
   constexpr float inv = 1.0f / ((float)N * (float)N);
   if (!active) return;
 #pragma unroll
   for (int i = 0; i < E; ++i) {
-    const float m = __ldg(&mod[coff + (size_t)i * T * N]);
     const float p2 = v[i].x * v[i].x + v[i].y * v[i].y;
     if (p2 > 0.f) {
       const float rs = rsqrtf(p2);
       if (want_err) {
-        const float d = p2 * rs - m;
+        const float d = p2 * rs - m[i];
         e2 = fma((double)d, (double)d, e2);
         e1 += fabs((double)d);
       }
-      const float sc = m * rs * inv;
+      const float sc = m[i] * rs * inv;
       v[i] = make_float2(v[i].x * sc, v[i].y * sc);
     } else {
       // the reference divides by |F| = 0 here (phasing_fourier.cl:14); keep M, zero phase
       if (want_err) {
-        e2 = fma((double)m, (double)m, e2);
-        e1 += (double)m;
+        e2 = fma((double)m[i], (double)m[i], e2);
+        e1 += (double)m[i];
       }
-      v[i] = make_float2(m * inv, 0.f);
+      v[i] = make_float2(m[i] * inv, 0.f);
     }
   }
 }
 
 template <int N, int E>
 __device__ __forceinline__ void col_item(const Slot& s, int step, int block, float2* smem,
-                                         const float2* __restrict__ tw_all, double* red) {
+                                         const float2* __restrict__ tw, double* red) {
   constexpr int T = N / E;
   constexpr int C = lines_per_item(N, E);
   constexpr float inv = 1.0f / ((float)N * (float)N);
-  const float2* __restrict__ tw = tw_all + N;
   const int tid = threadIdx.x;
   const int c = tid % C;
   const int t = tid / C;
@@ -302,9 +365,26 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   const BlockSync sync{};
   const size_t coff = (size_t)(active ? t : 0) * N + col;  // element (t + i*T, col) at coff + i*T*N
 
+  using SM = ColSmem<N, E>;
+  const float* mod_s = reinterpret_cast<const float*>(smem + SM::kMod) + (active ? t : 0) * C + c;
+  auto stage_modulus = [&]() {
+    // N rows x C floats of the modulus -> shared memory (row pitch C floats)
+    constexpr int RB = C * 4;
+    const float* src = s.modulus + (size_t)block * C;
+    float* dst = reinterpret_cast<float*>(smem + SM::kMod);
+    if constexpr (RB % 16 == 0) {
+      cp_async_rows(dst, src, N, RB, (size_t)N * 4, RB);
+    } else {
+      for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(dst + q * C, src + (size_t)q * N);
+    }
+  };
   float2 v[E];
+  float m[E];
   if (step == 0) {
     if (s.init != SP_INIT_RANDOM_PHASE) return;  // uniform over the block
+    stage_modulus();
+    cp_async_wait_all();
+    __syncthreads();
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -313,8 +393,8 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
         const float u = (float)(h >> 8) * (1.0f / 16777216.0f);
         float sn, cs;
         sincospif(2.0f * u, &sn, &cs);
-        const float m = __ldg(&s.modulus[coff + (size_t)i * T * N]) * inv;
-        v[i] = make_float2(m * cs, m * sn);
+        const float mm = mod_s[i * T * C] * inv;
+        v[i] = make_float2(mm * cs, mm * sn);
       }
     }
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);
@@ -328,21 +408,33 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   const bool dm = slot_alg(s, step) == SP_DM;
   const bool want_err = s.err != nullptr;
   double e2 = 0.0, e1 = 0.0;
+  stage_modulus();
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + coff + (size_t)i * T * N);
+  }
   for (int plane = 0; plane < (dm ? 2 : 1); ++plane) {
     float2* g = plane ? s.g2 : s.g;
-    if (active) {
+    if (plane && active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = g[coff + (size_t)i * T * N];
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(g + coff + (size_t)i * T * N);
     }
     fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-    project_cols<N, E>(v, s.modulus, coff, active, e2, e1, want_err && plane == 0);
+    if (plane == 0) {
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) m[i] = mod_s[i * T * C];
+    }
+    project_cols<N, E>(v, m, active, e2, e1, want_err && plane == 0);
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) g[coff + (size_t)i * T * N] = v[i];
     }
   }
-  (void)inv;
   if (want_err) {
     // block reduction of the two FP64 partial sums, one atomic each per item
 #pragma unroll
@@ -369,9 +461,15 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   }
 }
 
-// shared-memory entries one item needs (rows: L padded strips; cols: padded tile)
+// shared-memory entries one item needs (rows: L padded strips; cols: padded
+// tile), plus the N-entry twiddle table
 __host__ __device__ constexpr int item_smem_elems(int N, int E) {
   return lines_per_item(N, E) * pad32(N);
+}
+template <int N, int E>
+__host__ __device__ constexpr int pass_smem_elems() {
+  return RowSmem<N, E>::kTotal > ColSmem<N, E>::kTotal ? RowSmem<N, E>::kTotal
+                                                       : ColSmem<N, E>::kTotal;
 }
 
 }  // namespace sp

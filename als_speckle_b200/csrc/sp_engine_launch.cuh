@@ -23,13 +23,27 @@ __device__ __forceinline__ void load_slot(Slot* dst, const Slot* __restrict__ sr
   for (int w = threadIdx.x; w < (int)(sizeof(Slot) / 4); w += blockDim.x) d[w] = s[w];
 }
 
-constexpr int min_blocks_for(int E) { return E >= 32 ? 2 : 3; }
+// E = 32 keeps 64 registers of line data per thread plus the prefetched
+// psi/support: one 256-thread CTA per SM with up to 255 registers.  E = 16
+// halves that and runs two CTAs per SM.
+constexpr int min_blocks_for(int E) { return E >= 32 ? 1 : 2; }
+
+// Stage the N-entry twiddle table of this size in shared memory (once per
+// persistent CTA); returns its address.
+template <int N, int E>
+__device__ __forceinline__ const float2* stage_twiddles(float2* smem, const float2* __restrict__ tw_all) {
+  float2* tw = smem + item_smem_elems(N, E);  // = RowSmem::kTw = ColSmem::kTw
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_all[N + i];
+  __syncthreads();
+  return tw;
+}
 
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) row_pass_kernel(PassArgs a) {
   extern __shared__ float2 smem[];
   __shared__ Slot s;
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
+  const float2* tw = stage_twiddles<N, E>(smem, a.tw);
   for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
     const Item item = a.items[it];
     __syncthreads();  // previous item is done with smem and s
@@ -37,7 +51,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) row_pass_kernel(P
     __syncthreads();
     const int step = tick - s.start_tick;
     if (step < 0 || step > s.n_iter) continue;
-    row_item<N, E>(s, step, item.block, smem, a.tw);
+    row_item<N, E>(s, step, item.block, smem, tw);
   }
 }
 
@@ -47,6 +61,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) col_pass_kernel(P
   __shared__ Slot s;
   __shared__ double red[2 * kThreads / 32];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
+  const float2* tw = stage_twiddles<N, E>(smem, a.tw);
   for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
     const Item item = a.items[it];
     __syncthreads();
@@ -54,13 +69,13 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) col_pass_kernel(P
     __syncthreads();
     const int step = tick - s.start_tick;
     if (step < 0 || step > s.n_iter) continue;
-    col_item<N, E>(s, step, item.block, smem, a.tw, red);
+    col_item<N, E>(s, step, item.block, smem, tw, red);
   }
 }
 
 template <int N, int E>
 cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& a) {
-  const size_t sm = (size_t)item_smem_elems(N, E) * sizeof(float2);
+  const size_t sm = (size_t)pass_smem_elems<N, E>() * sizeof(float2);
   if (which == 0)
     col_pass_kernel<N, E><<<grid, kThreads, sm, st>>>(a);
   else
@@ -70,7 +85,7 @@ cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& 
 
 template <int N, int E>
 cudaError_t pass_setup_t(int* occupancy) {
-  const int sm = item_smem_elems(N, E) * (int)sizeof(float2);
+  const int sm = pass_smem_elems<N, E>() * (int)sizeof(float2);
   cudaError_t e;
   e = cudaFuncSetAttribute(col_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;

@@ -153,22 +153,35 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
     constexpr int M = E / R;                        // butterflies per thread
     constexpr bool LAST = (NS * R == N);
     constexpr int TWS = N / (NS * R);               // table stride for W_{NS*R}
-    // read this stage's inputs: element t + i*T -> v[i]
-    if (active) {
+    if constexpr (!LAST) {
+      // read all of this stage's inputs (element t + i*T -> v[i]) before
+      // anyone overwrites the buffer with this stage's outputs
+      if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+        for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+      }
+      sync();
     }
-    if constexpr (!LAST) sync();  // everyone has read before anyone overwrites
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const int j = t + m * T;
       const int k = j & (NS - 1);
       float2 u[R];
+      if constexpr (LAST) {
+        // the last stage writes nothing back to shared memory, so each
+        // butterfly reads its own inputs just before use (short live ranges)
+        asm volatile("" ::: "memory");
+        if (active) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) u[r] = v[m + r * M];
+          for (int r = 0; r < R; ++r) u[r] = lay.at(t + (m + r * M) * T);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = v[m + r * M];
+      }
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const float2 w = __ldg(&tw[(r * k) * TWS]);
+        const float2 w = tw[(r * k) * TWS];
         u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
       }
       dft<R, DIR>(u);
