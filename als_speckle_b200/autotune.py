@@ -1,8 +1,9 @@
 """Autotuner for the engine's per-size launch parameters.
 
 For a size N it times, on the current device, the fused iteration for every
-values-per-thread choice E (16 or 32: the radix of the in-register first
-Stockham stage and the tile each CTA owns) and for several L2 group sizes
+values-per-thread choice E (8, 16 or 32: the radix of the in-register first
+Stockham stage, the tile each CTA owns and, through registers, how many CTAs
+share an SM) and for several L2 group sizes
 (trials whose planes are kept L2-resident together), and keeps the fastest.
 Results are cached in ``autotune.json`` next to this file, keyed by device
 name and N.
@@ -82,9 +83,9 @@ def tune(N, trials=None, iters=60, path=CACHE, verbose=True):
     plane = N * N * 8
     if trials is None:
         trials = max(1, min(128, (1 << 30) // (3 * plane)))
-    groups = sorted({g for g in (4, 8, 12, 16, 24, 32, trials) if g <= trials})
+    groups = sorted({g for g in (8, 16, 32, trials) if g <= trials})
     results = []
-    for E in (16, 32):
+    for E in (8, 16, 32):
         for g in groups:
             l2 = g * 2 * plane if g < trials else 0
             rate = _time_config(N, E, l2, trials, iters)

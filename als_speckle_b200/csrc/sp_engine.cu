@@ -51,9 +51,10 @@ static cudaError_t pass_setup(int N, int E, int* occ) {
   }
 }
 
-// Per device, per (logN, E): dynamic-smem attribute set and occupancy cached.
+// Per device, per (logN, E): dynamic-smem attributes set and the resident CTAs
+// per SM of the column pass ([0]) and row pass ([1]) cached.
 static std::mutex g_setup_mutex;
-static int g_occ[64][13][2];  // 0 = not yet configured
+static int g_occ[64][13][3][2];  // [device][log2 N][E = 8, 16, 32][pass]; 0 = not yet configured
 static int g_sms[64];
 
 static cudaError_t occupancy_for(int N, int E, int* occ, int* sms) {
@@ -61,24 +62,27 @@ static cudaError_t occupancy_for(int N, int E, int* occ, int* sms) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  const int l = ilog2(N), k = (E >= 32 ? 1 : 0);
+  const int l = ilog2(N), k = (E >= 32 ? 2 : (E >= 16 ? 1 : 0));
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (g_sms[dev] == 0) {
     e = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
   }
-  if (g_occ[dev][l][k] == 0) {
-    int o = 0;
-    e = pass_setup(N, E, &o);
+  if (g_occ[dev][l][k][0] == 0) {
+    int o[2] = {0, 0};
+    e = pass_setup(N, E, o);
     if (e != cudaSuccess) return e;
-    g_occ[dev][l][k] = std::max(1, o);
+    g_occ[dev][l][k][0] = std::max(1, o[0]);
+    g_occ[dev][l][k][1] = std::max(1, o[1]);
   }
-  *occ = g_occ[dev][l][k];
+  occ[0] = g_occ[dev][l][k][0];
+  occ[1] = g_occ[dev][l][k][1];
   *sms = g_sms[dev];
   return cudaSuccess;
 }
 
 constexpr size_t kAlign = 256;
+constexpr int kMinE = 8;  // smallest values-per-thread choice (most work items)
 static inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 static bool uses_dm(const sp_trial& t) {
@@ -144,7 +148,7 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
   int items = 0;
   for (int i = 0; i < n; ++i) {
     const int N = trials[i].n;
-    items += N / lines_per_item(N, effective_e(N, 16));
+    items += N / lines_per_item(N, effective_e(N, kMinE));
   }
   L.n_items = items;
   L.planes_off = L.items_off + align_up(sizeof(Item) * (size_t)std::max(items, 1));
@@ -167,7 +171,7 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
 
 // one launch target: the items of one size within one group
 struct Segment {
-  int N, E, first, count, grid;
+  int N, E, first, count, grid[2];  // grid[pass]: 0 column, 1 row
 };
 
 struct GraphKey {
@@ -189,7 +193,7 @@ static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, con
     for (int which = 0; which < 2; ++which) {
       for (const Segment& sg : segs) {
         PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw};
-        SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid, st, a));
+        SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid[which], st, a));
       }
     }
   }
@@ -263,11 +267,15 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       }
       const int count = (int)hi.size() - first;
       if (count == 0) continue;
-      int occ = 1, sms = 1;
-      SP_CUDA_TRY(occupancy_for(N, E, &occ, &sms));
-      int per_sm = occ;
-      if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
-      segs[g].push_back(Segment{N, E, first, count, std::max(1, std::min(count, sms * per_sm))});
+      int occ[2] = {1, 1}, sms = 1;
+      SP_CUDA_TRY(occupancy_for(N, E, occ, &sms));
+      Segment sg{N, E, first, count, {1, 1}};
+      for (int p = 0; p < 2; ++p) {
+        int per_sm = occ[p];
+        if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
+        sg.grid[p] = std::max(1, std::min(count, sms * per_sm));
+      }
+      segs[g].push_back(sg);
     }
     for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
       const sp_trial& t = trials[i];
@@ -303,6 +311,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       s.err = t.errors_dev;
     }
   }
+  SP_CHECK((int)hi.size() <= L.n_items, SP_ERR_INVALID,
+           "internal: %zu work items exceed the %d reserved", hi.size(), L.n_items);
   SP_CUDA_TRY(cudaMemcpyAsync(ws + L.slots_off, hs.data(), sizeof(Slot) * hs.size(),
                               cudaMemcpyHostToDevice, st));
   if (!hi.empty())
@@ -326,7 +336,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       continue;
     }
     GraphKey key{workspace_dev, dev, g, ticks[g], {}};
-    for (const Segment& sg : segs[g]) key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid});
+    for (const Segment& sg : segs[g])
+      key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1]});
     cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);

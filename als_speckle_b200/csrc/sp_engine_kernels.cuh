@@ -117,11 +117,7 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t seed, uint32_t trial, uint
 // Streaming loads.  Pixel data is read once per pass, so it bypasses L1
 // (keeping L1 for nothing else is pointless: twiddles live in shared memory).
 // Read-only inputs (modulus, support) also take the non-coherent path.
-__device__ __forceinline__ float2 ld_stream(const float2* p) {
-  float2 v;
-  asm volatile("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
-  return v;
-}
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_ro(const float* p) {
   float v;
   asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
@@ -160,9 +156,9 @@ __device__ __forceinline__ void cp_async_rows(void* sdst, const void* gsrc, int 
 template <int N, int E>
 struct RowSmem {
   static constexpr int L = lines_per_item(N, E);
-  static constexpr int kX = L * pad32(N);         // float2 entries
-  static constexpr int kTw = kX;                   // offset of the twiddle table
-  static constexpr int kPsi = kTw + N;
+  static constexpr int kX = L * padk(N, pad_shift(E));  // float2 entries
+  static constexpr int kTw = kX;                         // offset of the twiddle tables
+  static constexpr int kPsi = kTw + tw_stage_total(N, E);
   static constexpr int kSupPitch = N + 16;         // floats per support row
   static constexpr int kSup = kPsi + L * N;        // offset (float2 units)
   static constexpr int kTotal = kSup + (L * kSupPitch + 1) / 2;
@@ -170,9 +166,9 @@ struct RowSmem {
 template <int N, int E>
 struct ColSmem {
   static constexpr int C = lines_per_item(N, E);
-  static constexpr int kX = C * pad32(N);
+  static constexpr int kX = C * padk(N, pad_shift(E));
   static constexpr int kTw = kX;
-  static constexpr int kMod = kTw + N;             // N rows x C floats
+  static constexpr int kMod = kTw + tw_stage_total(N, E);  // N rows x C floats
   static constexpr int kTotal = kMod + (N * C + 1) / 2;
 };
 
@@ -189,12 +185,14 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
   using Sync = typename std::conditional<(T <= 32), WarpSync, BlockSync>::type;
+  constexpr int SH = pad_shift(E);
+  constexpr bool kFull = (L * T == kThreads);  // every thread owns a line segment
   const int tid = threadIdx.x;
   const int lrow = tid / T;
   const int t = tid - lrow * T;
-  const bool active = lrow < L;
+  const bool active = kFull || lrow < L;
   const int row = block * L + (active ? lrow : 0);
-  const RowLayout lay{smem + (active ? lrow : 0) * pad32(N)};
+  const RowLayout<SH> lay{smem + (active ? lrow : 0) * padk(N, SH)};
   const Sync sync{};
   const float b = s.beta;
   const size_t roff = (size_t)row * N + t;
@@ -322,31 +320,30 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
 // ---------------------------------------------------------------------------
 // column pass for one item of a size-N slot
 // ---------------------------------------------------------------------------
+// m_s[i * mstride] is the modulus of element i (shared memory)
 template <int N, int E>
-__device__ __forceinline__ void project_cols(float2 (&v)[E], const float (&m)[E], bool active,
-                                             double& e2, double& e1, bool want_err) {
+__device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, int mstride,
+                                             bool active, double& e2, double& e1, bool want_err) {
   constexpr float inv = 1.0f / ((float)N * (float)N);
   if (!active) return;
+  // per-thread partial sums of E terms in FP32, accumulated into FP64
+  float f2 = 0.f, f1 = 0.f;
+  float m[E];
 #pragma unroll
   for (int i = 0; i < E; ++i) {
+    m[i] = m_s[i * mstride];
     const float p2 = v[i].x * v[i].x + v[i].y * v[i].y;
-    if (p2 > 0.f) {
-      const float rs = rsqrtf(p2);
-      if (want_err) {
-        const float d = p2 * rs - m[i];
-        e2 = fma((double)d, (double)d, e2);
-        e1 += fabs((double)d);
-      }
-      const float sc = m[i] * rs * inv;
-      v[i] = make_float2(v[i].x * sc, v[i].y * sc);
-    } else {
-      // the reference divides by |F| = 0 here (phasing_fourier.cl:14); keep M, zero phase
-      if (want_err) {
-        e2 = fma((double)m[i], (double)m[i], e2);
-        e1 += (double)m[i];
-      }
-      v[i] = make_float2(m[i] * inv, 0.f);
-    }
+    const float rs = p2 > 0.f ? rsqrtf(p2) : 0.f;
+    const float d = p2 * rs - m[i];  // |F| - M (|F| = 0 gives -M)
+    f2 = fmaf(d, d, f2);
+    f1 += fabsf(d);
+    // the reference divides by |F| = 0 (phasing_fourier.cl:14); keep M, zero phase
+    const float sc = m[i] * rs * inv;
+    v[i] = p2 > 0.f ? make_float2(v[i].x * sc, v[i].y * sc) : make_float2(m[i] * inv, 0.f);
+  }
+  if (want_err) {
+    e2 += (double)f2;
+    e1 += (double)f1;
   }
 }
 
@@ -356,12 +353,13 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   constexpr int T = N / E;
   constexpr int C = lines_per_item(N, E);
   constexpr float inv = 1.0f / ((float)N * (float)N);
+  constexpr bool kFull = (C * T == kThreads);
   const int tid = threadIdx.x;
   const int c = tid % C;
   const int t = tid / C;
-  const bool active = t < T;
+  const bool active = kFull || t < T;
   const int col = block * C + c;
-  const ColLayout lay{smem, C, c};
+  const ColLayout<pad_shift(E), C> lay{smem + c};
   const BlockSync sync{};
   const size_t coff = (size_t)(active ? t : 0) * N + col;  // element (t + i*T, col) at coff + i*T*N
 
@@ -379,7 +377,6 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
     }
   };
   float2 v[E];
-  float m[E];
   if (step == 0) {
     if (s.init != SP_INIT_RANDOM_PHASE) return;  // uniform over the block
     stage_modulus();
@@ -424,11 +421,7 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
       cp_async_wait_all();
       __syncthreads();
     }
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) m[i] = mod_s[i * T * C];
-    }
-    project_cols<N, E>(v, m, active, e2, e1, want_err && plane == 0);
+    project_cols<N, E>(v, mod_s, T * C, active, e2, e1, want_err && plane == 0);
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);
     if (active) {
 #pragma unroll
@@ -461,10 +454,10 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   }
 }
 
-// shared-memory entries one item needs (rows: L padded strips; cols: padded
-// tile), plus the N-entry twiddle table
+// shared-memory entries of one item's exchange buffer (rows: L padded strips;
+// cols: padded tile)
 __host__ __device__ constexpr int item_smem_elems(int N, int E) {
-  return lines_per_item(N, E) * pad32(N);
+  return lines_per_item(N, E) * padk(N, pad_shift(E));
 }
 template <int N, int E>
 __host__ __device__ constexpr int pass_smem_elems() {

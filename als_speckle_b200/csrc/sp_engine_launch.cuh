@@ -26,20 +26,28 @@ __device__ __forceinline__ void load_slot(Slot* dst, const Slot* __restrict__ sr
 // E = 32 keeps 64 registers of line data per thread plus the prefetched
 // psi/support: one 256-thread CTA per SM with up to 255 registers.  E = 16
 // halves that and runs two CTAs per SM.
-constexpr int min_blocks_for(int E) { return E >= 32 ? 1 : 2; }
+// smallest E instantiated for size N (8, or N/256 when a line needs more threads)
+constexpr int kSmallE(int N) { return (N / kThreads > 8) ? N / kThreads : (N >= 8 ? 8 : N); }
 
-// Stage the N-entry twiddle table of this size in shared memory (once per
-// persistent CTA); returns its address.
+// Resident CTAs per SM each kernel is compiled for (registers per thread =
+// 64K / (256 * this)): E = 32 needs ~240 registers, E = 16 fits 128 and E = 8
+// fits 64 (four CTAs, 32 warps per SM).
+constexpr int min_blocks_for(int E, bool row) {
+  return E >= 32 ? 1 : (E >= 16 ? 2 : 4);
+}
+
+// Build this size's per-stage twiddle tables in shared memory (once per
+// persistent CTA); returns their address.
 template <int N, int E>
 __device__ __forceinline__ const float2* stage_twiddles(float2* smem, const float2* __restrict__ tw_all) {
   float2* tw = smem + item_smem_elems(N, E);  // = RowSmem::kTw = ColSmem::kTw
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_all[N + i];
+  build_stage_twiddles<N, E>(tw, tw_all + N);
   __syncthreads();
   return tw;
 }
 
 template <int N, int E>
-__global__ void __launch_bounds__(kThreads, min_blocks_for(E)) row_pass_kernel(PassArgs a) {
+__global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_kernel(PassArgs a) {
   extern __shared__ float2 smem[];
   __shared__ Slot s;
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
@@ -56,7 +64,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) row_pass_kernel(P
 }
 
 template <int N, int E>
-__global__ void __launch_bounds__(kThreads, min_blocks_for(E)) col_pass_kernel(PassArgs a) {
+__global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_kernel(PassArgs a) {
   extern __shared__ float2 smem[];
   __shared__ Slot s;
   __shared__ double red[2 * kThreads / 32];
@@ -74,30 +82,31 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E)) col_pass_kernel(P
 }
 
 template <int N, int E>
+constexpr size_t col_smem_bytes() { return (size_t)ColSmem<N, E>::kTotal * sizeof(float2); }
+template <int N, int E>
+constexpr size_t row_smem_bytes() { return (size_t)RowSmem<N, E>::kTotal * sizeof(float2); }
+
+template <int N, int E>
 cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& a) {
-  const size_t sm = (size_t)pass_smem_elems<N, E>() * sizeof(float2);
   if (which == 0)
-    col_pass_kernel<N, E><<<grid, kThreads, sm, st>>>(a);
+    col_pass_kernel<N, E><<<grid, kThreads, col_smem_bytes<N, E>(), st>>>(a);
   else
-    row_pass_kernel<N, E><<<grid, kThreads, sm, st>>>(a);
+    row_pass_kernel<N, E><<<grid, kThreads, row_smem_bytes<N, E>(), st>>>(a);
   return cudaGetLastError();
 }
 
+// occupancy[0] = resident column-pass CTAs per SM, occupancy[1] = row-pass
 template <int N, int E>
 cudaError_t pass_setup_t(int* occupancy) {
-  const int sm = pass_smem_elems<N, E>() * (int)sizeof(float2);
+  const int sc = (int)col_smem_bytes<N, E>(), sr = (int)row_smem_bytes<N, E>();
   cudaError_t e;
-  e = cudaFuncSetAttribute(col_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  e = cudaFuncSetAttribute(col_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(row_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  e = cudaFuncSetAttribute(row_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
   if (e != cudaSuccess) return e;
-  int a = 0, b = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, col_pass_kernel<N, E>, kThreads, sm);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[0], col_pass_kernel<N, E>, kThreads, sc);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, row_pass_kernel<N, E>, kThreads, sm);
-  if (e != cudaSuccess) return e;
-  *occupancy = a < b ? a : b;
-  return cudaSuccess;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[1], row_pass_kernel<N, E>, kThreads, sr);
 }
 
 // Per-size entry points (defined in sp_engine_n<N>.cu).  E is clamped to N.
@@ -118,17 +127,21 @@ SP_DECLARE_SIZE(4096)
 #define SP_DEFINE_SIZE(N)                                                                    \
   cudaError_t launch_pass_n##N(int E, int which, int grid, cudaStream_t st, const PassArgs& a) { \
     if (E >= 32 && N >= 32) return launch_pass_t<N, (N >= 32 ? 32 : N)>(which, grid, st, a);   \
-    return launch_pass_t<N, (N >= 16 ? 16 : N)>(which, grid, st, a);                           \
+    if (E >= 16 && N >= 16) return launch_pass_t<N, (N >= 16 ? 16 : N)>(which, grid, st, a);   \
+    return launch_pass_t<N, kSmallE(N)>(which, grid, st, a);                                  \
   }                                                                                          \
   cudaError_t pass_setup_n##N(int E, int* occupancy) {                                       \
     if (E >= 32 && N >= 32) return pass_setup_t<N, (N >= 32 ? 32 : N)>(occupancy);            \
-    return pass_setup_t<N, (N >= 16 ? 16 : N)>(occupancy);                                    \
+    if (E >= 16 && N >= 16) return pass_setup_t<N, (N >= 16 ? 16 : N)>(occupancy);            \
+    return pass_setup_t<N, kSmallE(N)>(occupancy);                                            \
   }
 
-// E actually used for a requested E at size N
+// E actually used for a requested E at size N: 32, 16 or 8, at most N, and at
+// least N/256 so that a line needs no more than the CTA's 256 threads
 inline int effective_e(int N, int E) {
-  if (E >= 32 && N >= 32) return 32;
-  return N >= 16 ? 16 : N;
+  int e = (E >= 32 && N >= 32) ? 32 : ((E >= 16 && N >= 16) ? 16 : (N >= 8 ? 8 : N));
+  while (N / e > kThreads) e *= 2;
+  return e;
 }
 
 }  // namespace sp

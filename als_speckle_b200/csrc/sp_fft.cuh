@@ -120,21 +120,71 @@ __device__ __forceinline__ void dft(float2* v) {
   }
 }
 
+// Shared-memory padding: one spare slot per 2^SH entries.  SH = 5 for E = 32
+// and SH = 4 for E <= 16 make every exchange of both layouts conflict-free for
+// 8-byte accesses (checked against a bank model for N = 64..2048).
+__host__ __device__ constexpr int pad_shift(int E) { return E >= 32 ? 5 : 4; }
+__host__ __device__ __forceinline__ constexpr int padk(int a, int sh) { return a + (a >> sh); }
 __host__ __device__ __forceinline__ constexpr int pad32(int a) { return a + (a >> 5); }
 
 // Shared-memory layouts for a Stockham index a in [0, N).
 // Rows: each line owns a contiguous padded strip.
+// `at(a)` takes a Stockham index; `atp(p)` an index already padded, which lets
+// callers build addresses as a per-thread base plus compile-time constants
+// (padk(x + m 2^SH) = padk(x) + m (2^SH + 1)).
+template <int SH>
 struct RowLayout {
+  static constexpr int kShift = SH;
   float2* base;
-  __device__ __forceinline__ float2& at(int a) const { return base[pad32(a)]; }
+  __device__ __forceinline__ float2& at(int a) const { return base[padk(a, SH)]; }
+  __device__ __forceinline__ float2& atp(int p) const { return base[p]; }
 };
 // Column tiles: C lines interleaved element by element (line c is the column).
+template <int SH, int C>
 struct ColLayout {
-  float2* base;
-  int C;
-  int c;
-  __device__ __forceinline__ float2& at(int a) const { return base[pad32(a) * C + c]; }
+  static constexpr int kShift = SH;
+  float2* base;  // already offset by the column index c
+  __device__ __forceinline__ float2& at(int a) const { return base[padk(a, SH) * C]; }
+  __device__ __forceinline__ float2& atp(int p) const { return base[p * C]; }
 };
+
+// Twiddles of every Stockham stage after the first, stored per stage as
+// [r][k] = W_{NS*R}^(r*k) (r < R, k < NS), so that adjacent threads (adjacent
+// k) read adjacent entries.  Offset of the table of the stage that starts
+// with sub-transform size NS:
+__host__ __device__ constexpr int tw_stage_offset(int N, int E, int NS_target) {
+  int off = 0;
+  for (int NS = E; NS < NS_target && NS < N;) {
+    const int R = (N / NS) < E ? (N / NS) : E;
+    off += R * NS;
+    NS *= R;
+  }
+  return off;
+}
+__host__ __device__ constexpr int tw_stage_total(int N, int E) { return tw_stage_offset(N, E, N); }
+
+// Build the stage tables of (N, E) at `dst` (shared memory) from the N-entry
+// table tw_n[x] = exp(-2 pi i x / N).  All threads of the block take part;
+// the caller synchronises afterwards.
+template <int N, int E>
+__device__ __forceinline__ void build_stage_twiddles(float2* dst, const float2* __restrict__ tw_n) {
+  constexpr int total = tw_stage_total(N, E);
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    int off = 0, NS = E;
+    float2 w = make_float2(1.f, 0.f);
+    while (NS < N) {
+      const int R = (N / NS) < E ? (N / NS) : E;
+      if (q < off + R * NS) {
+        const int r = (q - off) / NS, k = (q - off) - r * NS;
+        w = tw_n[(r * k) * (N / (NS * R))];
+        break;
+      }
+      off += R * NS;
+      NS *= R;
+    }
+    dst[q] = w;
+  }
+}
 
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
@@ -148,17 +198,24 @@ template <int N, int E, int DIR, int NS, class Lay, class Sync>
 __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const Sync& sync,
                                            bool active, int t, const float2* __restrict__ tw) {
   constexpr int T = N / E;
+  constexpr int SH = Lay::kShift;
+  constexpr int P = 1 << SH;
   if constexpr (NS < N) {
     constexpr int R = (N / NS) < E ? (N / NS) : E;  // radix of this stage
     constexpr int M = E / R;                        // butterflies per thread
     constexpr bool LAST = (NS * R == N);
-    constexpr int TWS = N / (NS * R);               // table stride for W_{NS*R}
+    // element t + i*T: padded index padk(t) + i * TP when T is a multiple of P
+    constexpr bool LIN_RD = (T % P) == 0;
+    constexpr int TP = T + T / P;
+    const int prd = padk(t, SH);
+    auto rd = [&](int i) -> float2& { return LIN_RD ? lay.atp(prd + i * TP) : lay.at(t + i * T); };
+    const float2* __restrict__ tws = tw + tw_stage_offset(N, E, NS);  // this stage's [r][k] table
     if constexpr (!LAST) {
       // read all of this stage's inputs (element t + i*T -> v[i]) before
       // anyone overwrites the buffer with this stage's outputs
       if (active) {
 #pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+        for (int i = 0; i < E; ++i) v[i] = rd(i);
       }
       sync();
     }
@@ -170,10 +227,9 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
       if constexpr (LAST) {
         // the last stage writes nothing back to shared memory, so each
         // butterfly reads its own inputs just before use (short live ranges)
-        asm volatile("" ::: "memory");
         if (active) {
 #pragma unroll
-          for (int r = 0; r < R; ++r) u[r] = lay.at(t + (m + r * M) * T);
+          for (int r = 0; r < R; ++r) u[r] = rd(m + r * M);
         }
       } else {
 #pragma unroll
@@ -181,7 +237,7 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
       }
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const float2 w = tw[(r * k) * TWS];
+        const float2 w = tws[r * NS + k];
         u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
       }
       dft<R, DIR>(u);
@@ -189,10 +245,18 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
 #pragma unroll
         for (int r = 0; r < R; ++r) v[m + r * M] = u[r];
       } else {
+        // outputs at base + r*NS; NS >= E >= P is a multiple of P
         const int base = (j / NS) * NS * R + k;
+        const int pb = padk(base, SH);
+        constexpr int NSP = NS + NS / P;
         if (active) {
 #pragma unroll
-          for (int r = 0; r < R; ++r) lay.at(base + r * NS) = u[r];
+          for (int r = 0; r < R; ++r) {
+            if constexpr (NS % P == 0)
+              lay.atp(pb + r * NSP) = u[r];
+            else
+              lay.at(base + r * NS) = u[r];
+          }
         }
       }
     }
@@ -204,7 +268,8 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
 }
 
 // Full 1-D transform of one line held as v[i] = x[t + i*T]; on return
-// v[i] = X[t + i*T].  `tw` points at the N-entry table W_N^x = exp(-2 pi i x/N).
+// v[i] = X[t + i*T].  `tw` points at the stage tables built by
+// build_stage_twiddles<N, E>.
 // Every thread of the block must call this (it synchronises); inactive threads
 // pass active=false and skip all memory traffic.
 template <int N, int E, int DIR, class Lay, class Sync>
@@ -215,10 +280,18 @@ __device__ __forceinline__ void fft_line(float2 (&v)[E], const Lay& lay, const S
   dft<E, DIR>(v);
   if constexpr (T > 1) {
     // stage-1 outputs go to out[t*E + r]
+    constexpr int SH = Lay::kShift;
+    constexpr bool LIN_WR = (E % (1 << SH)) == 0;
+    const int pw = padk(t * E, SH);
     sync();  // previous readers of this shared buffer are done
     if (active) {
 #pragma unroll
-      for (int r = 0; r < E; ++r) lay.at(t * E + r) = v[r];
+      for (int r = 0; r < E; ++r) {
+        if constexpr (LIN_WR)
+          lay.atp(pw + r + (r >> SH)) = v[r];
+        else
+          lay.at(t * E + r) = v[r];
+      }
     }
     sync();
     fft_stages<N, E, DIR, E, Lay, Sync>(v, lay, sync, active, t, tw);

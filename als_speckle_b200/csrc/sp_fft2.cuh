@@ -14,13 +14,17 @@ __global__ void __launch_bounds__(kThreads) fft_rows_kernel(const float2* in,
   constexpr int E = (N < 16 ? N : 16);
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
+  constexpr int SH = pad_shift(E);
   using Sync = typename std::conditional<(T <= 32), WarpSync, BlockSync>::type;
   extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, tw_all + N);
+  __syncthreads();
   const int tid = threadIdx.x;
   const int lrow = tid / T;
   const int t = tid - lrow * T;
   const bool active = lrow < L;
-  const RowLayout lay{smem + (active ? lrow : 0) * pad32(N)};
+  const RowLayout<SH> lay{smem + (active ? lrow : 0) * padk(N, SH)};
   const int items = batch * (N / L);
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
     const size_t row = (size_t)it * L + (active ? lrow : 0);  // global row over the batch
@@ -30,7 +34,7 @@ __global__ void __launch_bounds__(kThreads) fft_rows_kernel(const float2* in,
 #pragma unroll
       for (int i = 0; i < E; ++i) v[i] = in[off + i * T];
     }
-    fft_line<N, E, DIR>(v, lay, Sync{}, active, t, tw_all + N);
+    fft_line<N, E, DIR>(v, lay, Sync{}, active, t, tw);
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) out[off + i * T] = v[i];
@@ -47,11 +51,14 @@ __global__ void __launch_bounds__(kThreads) fft_cols_kernel(const float2* in,
   constexpr int T = N / E;
   constexpr int C = lines_per_item(N, E);
   extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, tw_all + N);
+  __syncthreads();
   const int tid = threadIdx.x;
   const int c = tid % C;
   const int t = tid / C;
   const bool active = t < T;
-  const ColLayout lay{smem, C, c};
+  const ColLayout<pad_shift(E), C> lay{smem + c};
   const int per_plane = N / C;
   const int items = batch * per_plane;
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
@@ -64,7 +71,7 @@ __global__ void __launch_bounds__(kThreads) fft_cols_kernel(const float2* in,
 #pragma unroll
       for (int i = 0; i < E; ++i) v[i] = in[off + (size_t)i * T * N];
     }
-    fft_line<N, E, DIR>(v, lay, BlockSync{}, active, t, tw_all + N);
+    fft_line<N, E, DIR>(v, lay, BlockSync{}, active, t, tw);
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) out[off + (size_t)i * T * N] = make_float2(v[i].x * scale, v[i].y * scale);
@@ -76,7 +83,7 @@ template <int N>
 cudaError_t fft2_t(const float2* in, float2* out, int batch, int inverse, cudaStream_t st,
                    const float2* tw, int n_sms) {
   constexpr int E = (N < 16 ? N : 16);
-  const int sm = item_smem_elems(N, E) * (int)sizeof(float2);
+  const int sm = (item_smem_elems(N, E) + tw_stage_total(N, E)) * (int)sizeof(float2);
   const int rows_items = batch * (N / lines_per_item(N, E));
   const int grid = rows_items < n_sms * 4 ? rows_items : n_sms * 4;
   const float scale = inverse ? 1.0f / ((float)N * (float)N) : 1.0f;

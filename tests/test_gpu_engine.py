@@ -67,10 +67,14 @@ def test_single_projection_vs_reference_golden(engine, N, alg):
     assert rel(psi.cpu().numpy(), g["N%d_%s_psi_in" % (N, alg)]) < 1e-5
 
 
+@pytest.mark.parametrize("E", [8, 16, 32])
 @pytest.mark.parametrize("N", [128, 256, 512, 1024, 2048])
 @pytest.mark.parametrize("alg", ["hio", "er", "raar", "sf", "dm"])
-def test_single_projection_vs_fp64_oracle(engine, N, alg):
+def test_single_projection_vs_fp64_oracle(N, alg, E):
+    """One projection + update of every algorithm, for every values-per-thread
+    choice E, against the FP64 oracle; the FP64 error sums too."""
     from als_speckle_b200 import synth
+    from als_speckle_b200.engine import Engine
     obj, M, S = synth.pattern(N, n_ellipses=6, box=N // 4, peak=1e6, seed=N, support_edge=N // 4 + N // 16)
     rng = np.random.default_rng(1)
     psi0 = ((rng.random((N, N)) + 1j * rng.random((N, N))) * S).astype(np.complex64)
@@ -78,6 +82,7 @@ def test_single_projection_vs_fp64_oracle(engine, N, alg):
     want, _ = O.iteration(psi0, M, S, alg, beta, quirks="gpu", mode="f64")
     psi = dev(psi0)
     err = torch.zeros((1, 2), dtype=torch.float64, device="cuda")
+    engine = Engine(use_graph=False, e_per_n={N: E})
     engine.solve([_spec(psi, dev(M), dev(S), 1, ((alg, 1),), beta, errors=err)])
     assert rel(psi.cpu().numpy(), want) < 1e-5
     e, r = O.modulus_errors(psi0, M)
@@ -85,24 +90,26 @@ def test_single_projection_vs_fp64_oracle(engine, N, alg):
     got = err.cpu().numpy()[0]
     assert abs(got[0] / np.sum(m * m) - e) / e < 1e-5
     assert abs(got[1] / np.sum(m) - r) / r < 1e-5
+    engine.close()
 
 
 @pytest.mark.parametrize("N", [512])
 def test_projection_e16_equals_e32(N):
-    """Both per-thread radix choices give the same projection to FP32 rounding."""
+    """Per-thread radix choices give the same result to FP32 rounding."""
     from als_speckle_b200.engine import Engine
     from als_speckle_b200 import synth
     _, M, S = synth.pattern(N, n_ellipses=6, box=128, peak=1e6, seed=3, support_edge=160)
     rng = np.random.default_rng(2)
     psi0 = ((rng.random((N, N)) + 1j * rng.random((N, N))) * S).astype(np.complex64)
     outs = []
-    for E in (16, 32):
+    for E in (8, 16, 32):
         e = Engine(use_graph=False, e_per_n={N: E})
         psi = dev(psi0)
         e.solve([_spec(psi, dev(M), dev(S), 3, None, 0.9)])
         outs.append(psi.cpu().numpy())
         e.close()
-    assert rel(outs[0], outs[1]) < 1e-5
+    assert rel(outs[0], outs[2]) < 1e-5
+    assert rel(outs[1], outs[2]) < 1e-5
 
 
 def test_short_trajectories_vs_reference_golden(engine):
