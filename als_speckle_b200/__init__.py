@@ -1,4 +1,14 @@
-"""B200-native phase retrieval with the speckle.phasing API (dhparks/als_speckle)."""
-from . import engine, masking, phasing, synth  # noqa: F401
+"""B200-native phase retrieval with the speckle.phasing API (dhparks/als_speckle).
 
-__all__ = ["phasing", "engine", "masking", "synth"]
+Submodules load on first use, so ``python -m als_speckle_b200.build`` works
+before the library exists.
+"""
+import importlib
+
+__all__ = ["phasing", "engine", "masking", "synth", "serving", "distributed", "workloads"]
+
+
+def __getattr__(name):
+    if name in __all__:
+        return importlib.import_module("." + name, __name__)
+    raise AttributeError(name)

@@ -87,6 +87,8 @@ _SIGS = {
     "sp_prtf": ([_p, _i, _i, _i, _i, _p, _p, _p], _i),
     "sp_shrinkwrap": ([_p, _i, _i, _p, _p, _p, _i, _d, _d, _i, _p, _p, _p, _p, _p], _i),
     "sp_mean_frames": ([_p, _i, _i64, _p, _p], _i),
+    "sp_prtf_phasors": ([_p, _i, _i, _i, _i, _p, _p, _p], _i),
+    "sp_prtf_finish": ([_p, _i, _i, _p, _p], _i),
     "sp_xcorr_peak": ([_p, _p, _i, _i, _p, _p, _p], _i),
     "sp_roll": ([_p, _p, _i, _i, _i, _i, _p], _i),
     "sp_com_sums": ([_p, _i, _i, _i, _p, _p], _i),

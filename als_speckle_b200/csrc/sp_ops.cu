@@ -165,6 +165,36 @@ __global__ void prtf_accumulate_kernel(int frames, const float2* __restrict__ ff
   }
 }
 
+// sum_n F_n/|F_n| in FP32 (phasing_prtf_accumulate2.cl:20-23), added to acc
+__global__ void phasor_sum_kernel(int frames, const float2* __restrict__ fft, float2* __restrict__ acc,
+                                  int N) {
+  const int64_t NN = (int64_t)N * N;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < NN;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    float cr = 0.f, ci = 0.f;
+    for (int n = 0; n < frames; ++n) {
+      const float2 v = fft[k + n * NN];
+      const float h = hypotf(v.x, v.y);
+      if (h > 0.f) {
+        cr += v.x / h;
+        ci += v.y / h;
+      }
+    }
+    acc[k] = make_float2(acc[k].x + cr, acc[k].y + ci);
+  }
+}
+// prtf = fftshift(|acc| / frames)
+__global__ void prtf_finish_kernel(const float2* __restrict__ acc, int frames, float* __restrict__ prtf,
+                                   int N) {
+  const int64_t NN = (int64_t)N * N;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < NN;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(k / N), c = (int)(k - (int64_t)r * N);
+    const float2 a = acc[k];
+    prtf[(int64_t)((r + N / 2) % N) * N + (c + N / 2) % N] = hypotf(a.x / frames, a.y / frames);
+  }
+}
+
 // embed (n, rows, cols) frames at the corner of zeroed N x N planes
 __global__ void embed_kernel(const float2* __restrict__ src, float2* __restrict__ dst, int n,
                              int rows, int cols, int N) {
@@ -561,6 +591,33 @@ int sp_prtf(const void* frames, int n_frames, int rows, int cols, int N, void* w
   SP_CUDA_TRY(fft2_dispatch((const float2*)work, (float2*)work, N, n_frames, 0, st));
   prtf_accumulate_kernel<<<grid_for((int64_t)N * N), 256, 0, st>>>(n_frames, (const float2*)work,
                                                                    prtf, N, 1);
+  SP_CUDA_TRY(cudaGetLastError());
+  return SP_OK;
+}
+
+int sp_prtf_phasors(const void* frames, int n_frames, int rows, int cols, int N, void* work,
+                    void* acc, sp_stream_t stream) {
+  SP_CHECK(frames && work && acc && n_frames > 0, SP_ERR_INVALID, "sp_prtf_phasors: bad argument");
+  SP_CHECK(is_pow2(N) && N >= kMinN && N <= kMaxN, SP_ERR_SIZE, "sp_prtf_phasors: N=%d unsupported", N);
+  SP_CHECK(rows > 0 && cols > 0 && rows <= N && cols <= N, SP_ERR_INVALID,
+           "sp_prtf_phasors: frames larger than N");
+  cudaStream_t st = as_stream(stream);
+  const int64_t total = (int64_t)n_frames * N * N;
+  embed_kernel<<<grid_for(total), 256, 0, st>>>((const float2*)frames, (float2*)work, n_frames, rows,
+                                                cols, N);
+  SP_CUDA_TRY(cudaGetLastError());
+  SP_CUDA_TRY(fft2_dispatch((const float2*)work, (float2*)work, N, n_frames, 0, st));
+  phasor_sum_kernel<<<grid_for((int64_t)N * N), 256, 0, st>>>(n_frames, (const float2*)work,
+                                                              (float2*)acc, N);
+  SP_CUDA_TRY(cudaGetLastError());
+  return SP_OK;
+}
+
+int sp_prtf_finish(const void* acc, int n_frames, int N, float* prtf, sp_stream_t stream) {
+  SP_CHECK(acc && prtf && n_frames > 0, SP_ERR_INVALID, "sp_prtf_finish: bad argument");
+  SP_CHECK(is_pow2(N) && N >= kMinN && N <= kMaxN, SP_ERR_SIZE, "sp_prtf_finish: N=%d unsupported", N);
+  prtf_finish_kernel<<<grid_for((int64_t)N * N), 256, 0, as_stream(stream)>>>((const float2*)acc,
+                                                                             n_frames, prtf, N);
   SP_CUDA_TRY(cudaGetLastError());
   return SP_OK;
 }

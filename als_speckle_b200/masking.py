@@ -67,40 +67,50 @@ def label_parts(data, detect_val=(0.95, 1.05)):
     ``trace_object`` ``:271-377``) returns them.  Returns (labels int32, n);
     n counts empty parts (isolated pixels), whose label has no pixels.
     """
+    from scipy import ndimage
     data = np.asarray(data)
     mask = (data >= detect_val[0]) & (data <= detect_val[1])
-    R, Cc = mask.shape
-    parent = np.arange(R * Cc, dtype=np.int64)
+    R, C = mask.shape
+    lab, n = ndimage.label(mask, structure=np.ones((3, 3), bool))
+    if n == 0:
+        return np.zeros((R, C), np.int32), 0
+    # merge parts that touch across the periodic edges (rows 0/R-1, cols 0/C-1)
+    parent = np.arange(n + 1)
 
     def find(a):
-        root = a
-        while parent[root] != root:
-            root = parent[root]
-        while parent[a] != root:
-            parent[a], a = root, parent[a]
-        return root
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
 
-    idx = np.flatnonzero(mask.ravel())
-    for k in idx:
-        r, c = divmod(int(k), Cc)
-        for dr, dc in ((0, 1), (1, -1), (1, 0), (1, 1)):
-            rr, cc = (r + dr) % R, (c + dc) % Cc
-            if mask[rr, cc]:
-                a, b = find(int(k)), find(rr * Cc + cc)
-                if a != b:
-                    parent[max(a, b)] = min(a, b)
-    labels = np.zeros(R * Cc, np.int32)
-    order = {}
-    size = {}
-    for k in idx:
-        root = find(int(k))
-        size[root] = size.get(root, 0) + 1
-    for k in idx:
-        root = find(int(k))
-        if root not in order:
-            order[root] = len(order) + 1
-        # the flood fill never marks its start pixel itself, so a pixel with no
-        # neighbour in the mask is returned as an empty part (masking.py:357-372)
-        if size[root] > 1:
-            labels[k] = order[root]
-    return labels.reshape(R, Cc), len(order)
+    edges = []
+    top, bot = lab[0], lab[R - 1]
+    for dc in (-1, 0, 1):
+        edges.append((top, np.roll(bot, dc)))
+    left, right = lab[:, 0], lab[:, C - 1]
+    for dr in (-1, 0, 1):
+        edges.append((left, np.roll(right, dr)))
+    for a, b in edges:
+        both = (a > 0) & (b > 0)
+        for x, y in zip(a[both], b[both]):
+            rx, ry = find(int(x)), find(int(y))
+            if rx != ry:
+                parent[max(rx, ry)] = min(rx, ry)
+    roots = np.array([find(i) for i in range(n + 1)])
+    merged = roots[lab]
+    flat = merged.ravel()
+    # number parts by the raster position of their first pixel
+    ids, first = np.unique(flat, return_index=True)
+    keep = ids > 0
+    ids, first = ids[keep], first[keep]
+    order = ids[np.argsort(first)]
+    remap = np.zeros(n + 1, np.int32)
+    remap[order] = np.arange(1, len(order) + 1, dtype=np.int32)
+    out = remap[merged]
+    # the flood fill never marks its start pixel itself, so a pixel with no
+    # neighbour in the mask is returned as an empty part (masking.py:357-372)
+    sizes = np.bincount(out.ravel(), minlength=len(order) + 1)
+    single = sizes == 1
+    single[0] = False
+    out[single[out]] = 0
+    return out.astype(np.int32), len(order)

@@ -162,6 +162,13 @@ int sp_align_global_phase(void* frames_dev, int n_frames, int64_t frame_elems,
  * work_dev: complex64 n_frames*N*N scratch. */
 int sp_prtf(const void* frames_dev, int n_frames, int rows, int cols, int N, void* work_dev,
             float* prtf_dev, sp_stream_t stream);
+/* The two halves of sp_prtf, for PRTFs over frames spread across devices or
+ * calls: sp_prtf_phasors adds sum_n F_n/|F_n| (unshifted, complex64 N*N) of its
+ * frames into acc_dev; after the partial sums are added together,
+ * sp_prtf_finish writes fftshift(|acc|/n_frames) with n_frames the total count. */
+int sp_prtf_phasors(const void* frames_dev, int n_frames, int rows, int cols, int N, void* work_dev,
+                    void* acc_dev, sp_stream_t stream);
+int sp_prtf_finish(const void* acc_dev, int n_frames, int N, float* prtf_dev, sp_stream_t stream);
 /* refine_support (phasing.py:1747-1815) on a rows x cols crop: |avg| is blurred
  * by the circular separable kernel kr (rows) x kc (cols) in FP64 (the FFT
  * convolution with the fftshifted, normalised Gaussian is exactly this

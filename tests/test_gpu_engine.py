@@ -324,3 +324,18 @@ def test_plain_path_matches_engine():
               _lib.ptr(Md), _lib.ptr(Sd), _lib.ptr(work), _lib.stream_ptr())
     torch.cuda.synchronize()
     assert rel(a.cpu().numpy(), b.cpu().numpy()) < 1e-4
+
+
+def test_split_prtf_and_average_equal_one_shot():
+    """Partial phasor/frame sums over two halves, added and finished, equal
+    the PRTF and mean of all frames at once (the multi-GPU reduction path)."""
+    from als_speckle_b200.distributed import local_sums, finish_prtf
+    from als_speckle_b200.phasing import prtf, mean_frames
+    rng = np.random.default_rng(9)
+    fr = (rng.random((9, 20, 24)) * np.exp(1j * rng.normal(0, 0.4, (9, 20, 24)))).astype(np.complex64)
+    t = dev(fr)
+    f1, p1 = local_sums(t[:4], 32)
+    f2, p2 = local_sums(t[4:], 32)
+    got = finish_prtf(p1 + p2, 9).cpu().numpy()
+    assert np.allclose(got, prtf(t, N=32).cpu().numpy(), rtol=1e-5, atol=1e-6)
+    assert np.allclose(((f1 + f2) / 9).cpu().numpy(), mean_frames(t).cpu().numpy(), atol=1e-6)

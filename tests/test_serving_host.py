@@ -1,0 +1,98 @@
+"""Host logic of the continuous-batching service (no GPU: a fake engine)."""
+import numpy as np
+import torch
+
+from oracle import phasing_oracle as O
+
+
+class FakeEngine:
+    """Records each round's trials instead of launching kernels."""
+
+    def __init__(self):
+        self.calls = []
+
+    def solve(self, specs, stream=None):
+        self.calls.append([(s.n, s.iterations, s.random_phase, s.save is not None) for s in specs])
+        for s in specs:
+            s.psi += 1  # one mark per round
+            if s.save is not None:
+                s.save.fill_(s.psi.real.max().item())
+
+
+def _req(rid, N=16, iters=10, trials=2, arrival=0.0, order=(("hio", 3), ("er", 1))):
+    from als_speckle_b200.serving import Request
+    M = np.ones((N, N), np.float32)
+    S = np.zeros((N, N), np.float32)
+    S[4:12, 4:12] = 1
+    return Request(rid=rid, modulus=M, support=S, iterations=iters, trials=trials, order=order,
+                   arrival=arrival)
+
+
+def test_rotated_order_walks_the_cyclic_list():
+    from als_speckle_b200.serving import rotated_order
+    from als_speckle_b200.engine import expand_runs
+    order = (("hio", 5), ("er", 2), ("dm", 1))
+    algs, counts = expand_runs(order)
+    flat = [a for a, c in zip(algs, counts) for _ in range(c)]
+    names = O.expand_order(order)
+    for off in range(0, 17):
+        rot = rotated_order(flat, off)
+        got = [n for n, c in rot for _ in range(c)]
+        assert got == [names[(off + i) % len(names)] for i in range(len(names))]
+
+
+def test_rounds_chunks_and_first_chunk_random_start():
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    srv = ServingEngine(device="cpu", chunk=4, engine=eng)
+    srv.submit(_req(0, iters=10))
+    res = srv.run(realtime=False)
+    # 10 iterations in chunks of 4: 4, 4, 2; random start only in the first chunk
+    assert [c[0][1] for c in eng.calls] == [4, 4, 2]
+    assert [c[0][2] for c in eng.calls] == [True, False, False]
+    assert [c[0][3] for c in eng.calls] == [False, False, True]
+    assert res[0].save.shape[0] == 2 and srv.rounds == 3
+    assert srv.trial_iterations == 20
+
+
+def test_budget_admission_is_first_come_first_served():
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    one = _req(0).bytes_needed()
+    srv = ServingEngine(device="cpu", chunk=5, engine=eng, hbm_budget=int(one * 1.5))
+    for rid in range(3):
+        srv.submit(_req(rid, iters=10))
+    srv.run(realtime=False)
+    # only one request fits at a time: each round carries exactly one request's trials
+    assert all(len(c) == 2 for c in eng.calls)
+    assert len(eng.calls) == 6 and srv.in_use == 0
+
+
+def test_requests_join_as_others_finish():
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    srv = ServingEngine(device="cpu", chunk=5, engine=eng)
+    srv.submit(_req(0, iters=5, trials=1))
+    srv.submit(_req(1, iters=15, trials=3))
+    res = srv.run(realtime=False)
+    assert [len(c) for c in eng.calls] == [4, 3, 3]
+    assert set(res) == {0, 1}
+
+
+def test_oversize_request_rejected():
+    import pytest
+    from als_speckle_b200.serving import ServingEngine
+    srv = ServingEngine(device="cpu", engine=FakeEngine(), hbm_budget=1000)
+    with pytest.raises(ValueError):
+        srv.submit(_req(0))
+
+
+def test_poisson_workload_is_seeded():
+    from als_speckle_b200.serving import poisson_workload
+    a = poisson_workload(window=0.05, rate=200, sizes=(16, 32), probs=(0.5, 0.5), iters=(5, 9),
+                         trials=(1, 3), patterns_per_size=1)
+    b = poisson_workload(window=0.05, rate=200, sizes=(16, 32), probs=(0.5, 0.5), iters=(5, 9),
+                         trials=(1, 3), patterns_per_size=1)
+    assert [(r.n, r.iterations, r.trials, r.order, r.arrival) for r in a] == \
+        [(r.n, r.iterations, r.trials, r.order, r.arrival) for r in b]
+    assert all(np.diff([r.arrival for r in a]) > 0)
