@@ -82,6 +82,7 @@ class Result:
     arrival: float
     admitted: float
     finished: float
+    status: str = "done"      # "done", "diverged" (non-finite error sums) or "cancelled"
 
     @property
     def latency(self):
@@ -150,9 +151,36 @@ class ServingEngine:
             self.stream.synchronize()
 
     def submit(self, req: Request):
+        """Queue a request.  Rejected at once: a request larger than the
+        whole budget, or one whose modulus or support is not finite."""
         if req.bytes_needed() > self.budget:
             raise ValueError("request %d needs %d bytes, more than the whole budget" % (req.rid, req.bytes_needed()))
+        if not (np.all(np.isfinite(req.modulus)) and np.all(np.isfinite(req.support))):
+            raise ValueError("request %d: modulus and support must be finite" % req.rid)
+        if not np.any(req.support > 0):
+            raise ValueError("request %d: empty support" % req.rid)
         heapq.heappush(self.pending, (req.arrival, req.rid, req))
+
+    def cancel(self, rid: int):
+        """Drop a request whether it is waiting or in flight; its result is
+        recorded with status "cancelled" and its memory is released."""
+        for i, (_, r, req) in enumerate(self.pending):
+            if r == rid:
+                self.pending.pop(i)
+                heapq.heapify(self.pending)
+                self.results[rid] = Result(rid, np.zeros((0, 0, 0), np.complex64),
+                                           np.zeros((0, 0, 2)), (0, 0, 0, 0), req.arrival, -1.0, -1.0,
+                                           "cancelled")
+                return True
+        for a in self.active:
+            if a.req.rid == rid:
+                self.active.remove(a)
+                self.in_use -= a.bytes
+                self.results[rid] = Result(rid, np.zeros((0, 0, 0), np.complex64),
+                                           np.zeros((0, 0, 2)), a.box, a.req.arrival, a.admitted,
+                                           -1.0, "cancelled")
+                return True
+        return False
 
     def _admit(self, now):
         trials = sum(a.req.trials for a in self.active)
@@ -198,6 +226,14 @@ class ServingEngine:
             still = []
             for a, n in zip(self.active, steps):
                 a.done += n
+                if n and not bool(torch.isfinite(a.errors[:, a.done - 1]).all()):
+                    # the iterate has become non-finite: stop it and free its slots
+                    self.results[a.req.rid] = Result(
+                        a.req.rid, a.save.cpu().numpy(), a.errors.cpu().numpy(), a.box,
+                        a.req.arrival if realtime else 0.0, a.admitted if realtime else 0.0, t,
+                        "diverged")
+                    self.in_use -= a.bytes
+                    continue
                 if a.done >= a.req.iterations:
                     self.results[a.req.rid] = Result(
                         a.req.rid, a.save.cpu().numpy(), a.errors.cpu().numpy(), a.box,

@@ -96,3 +96,58 @@ def test_poisson_workload_is_seeded():
     assert [(r.n, r.iterations, r.trials, r.order, r.arrival) for r in a] == \
         [(r.n, r.iterations, r.trials, r.order, r.arrival) for r in b]
     assert all(np.diff([r.arrival for r in a]) > 0)
+
+
+def test_non_finite_and_empty_inputs_rejected():
+    import pytest
+    from als_speckle_b200.serving import ServingEngine
+    srv = ServingEngine(device="cpu", engine=FakeEngine())
+    bad = _req(0)
+    bad.modulus = bad.modulus.copy()
+    bad.modulus[3, 3] = np.nan
+    with pytest.raises(ValueError):
+        srv.submit(bad)
+    empty = _req(1)
+    empty.support = np.zeros_like(empty.support)
+    with pytest.raises(ValueError):
+        srv.submit(empty)
+
+
+class PoisonEngine(FakeEngine):
+    """Writes NaN error sums for one trial's request, as a diverging iterate would."""
+
+    def __init__(self, poison_n):
+        super().__init__()
+        self.poison_n = poison_n
+
+    def solve(self, specs, stream=None):
+        super().solve(specs, stream)
+        for s in specs:
+            if s.n == self.poison_n and s.errors is not None:
+                s.errors.fill_(float("nan"))
+
+
+def test_diverged_request_is_stopped_and_freed():
+    from als_speckle_b200.serving import ServingEngine
+    eng = PoisonEngine(poison_n=32)
+    srv = ServingEngine(device="cpu", chunk=4, engine=eng)
+    srv.submit(_req(0, N=16, iters=12))
+    srv.submit(_req(1, N=32, iters=12))
+    res = srv.run(realtime=False)
+    assert res[1].status == "diverged" and res[0].status == "done"
+    assert len(eng.calls) == 3 and [len(c) for c in eng.calls] == [4, 2, 2]
+    assert srv.in_use == 0
+
+
+def test_cancel_pending_and_active():
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    srv = ServingEngine(device="cpu", chunk=4, engine=eng)
+    srv.submit(_req(0, iters=8))
+    srv.submit(_req(1, iters=8, arrival=5.0))
+    assert srv.cancel(1) and not srv.cancel(7)
+    srv._admit(0.0)
+    assert srv.cancel(0) and srv.in_use == 0 and not srv.active
+    res = srv.run(realtime=False)
+    assert res[0].status == "cancelled" and res[1].status == "cancelled"
+    assert eng.calls == []
