@@ -137,67 +137,118 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Copy `rows` rows of `row_bytes` (a multiple of 16) starting at gsrc with
-// global row pitch gpitch bytes into shared memory with row pitch spitch bytes.
-__device__ __forceinline__ void cp_async_rows(void* sdst, const void* gsrc, int rows, int row_bytes,
-                                              size_t gpitch, int spitch) {
-  const int per_row = row_bytes >> 4;
-  const int chunks = rows * per_row;
-  for (int q = threadIdx.x; q < chunks; q += blockDim.x) {
-    const int r = q / per_row, c = q - r * per_row;
-    cp_async<16>(static_cast<char*>(sdst) + r * spitch + (c << 4),
-                 static_cast<const char*>(gsrc) + r * gpitch + (c << 4));
+// Copy ROWS rows of RB bytes (a multiple of 16) starting at gsrc with global
+// row pitch GP bytes into shared memory with row pitch SP bytes, 16 bytes per
+// cp.async.  All geometry is compile-time, so each thread's chunk addresses
+// are a base plus constants.
+template <int ROWS, int RB, int GP, int SP>
+__device__ __forceinline__ void cp_async_tile(void* sdst, const void* gsrc) {
+  static_assert(RB % 16 == 0 && SP % 16 == 0 && GP % 16 == 0, "16-byte chunks");
+  constexpr int PER_ROW = RB / 16;
+  constexpr int CHUNKS = ROWS * PER_ROW;
+  char* d = static_cast<char*>(sdst);
+  const char* g = static_cast<const char*>(gsrc);
+#pragma unroll
+  for (int j = 0; j < (CHUNKS + kThreads - 1) / kThreads; ++j) {
+    const int q = threadIdx.x + j * kThreads;
+    if (CHUNKS % kThreads == 0 || q < CHUNKS) {
+      const int r = q / PER_ROW, c = q - r * PER_ROW;  // PER_ROW is a power of two
+      cp_async<16>(d + r * SP + c * 16, g + (size_t)r * GP + c * 16);
+    }
   }
 }
 
 // Shared-memory plan of one pass item.  Row pass: exchange strips | twiddles |
 // psi tile (L x N complex) | support tile (L rows of N + 16 floats).  Column
 // pass: exchange tile | twiddles | modulus tile (N rows x C floats).
+// Row pass: two buffers of L padded strips that swap roles every item (one
+// holds the item's G rows and then serves as its exchange buffer, the other
+// receives its psi rows and, once the update has read them, the next item's
+// G rows) | twiddles | support tile (L rows of N + 16 floats).
 template <int N, int E>
 struct RowSmem {
   static constexpr int L = lines_per_item(N, E);
-  static constexpr int kX = L * padk(N, pad_shift(E));  // float2 entries
-  static constexpr int kTw = kX;                         // offset of the twiddle tables
-  static constexpr int kPsi = kTw + tw_stage_total(N, E);
-  static constexpr int kSupPitch = N + 16;         // floats per support row
-  static constexpr int kSup = kPsi + L * N;        // offset (float2 units)
+  // row pitch of both buffers: the padded line, rounded up to an even number
+  // of complex values so every row starts 16-byte aligned (cp.async)
+  static constexpr int kStrip = (padk(N, pad_shift(E)) + 1) & ~1;
+  static constexpr int kB = L * kStrip;                  // float2 entries per buffer
+  static constexpr int kTw = 2 * kB;                     // offset of the twiddle tables
+  static constexpr int kSupPitch = N + 16;               // floats per support row
+  static constexpr int kSup = kTw + tw_stage_total(N, E);  // offset (float2 units)
   static constexpr int kTotal = kSup + (L * kSupPitch + 1) / 2;
 };
+// Column pass: two tile buffers (the G tile of the next item is copied into
+// one while the other holds the current item, first as its G tile, then as
+// its exchange buffer) | twiddles | modulus tile (N rows x C floats).
 template <int N, int E>
 struct ColSmem {
   static constexpr int C = lines_per_item(N, E);
-  static constexpr int kX = C * padk(N, pad_shift(E));
-  static constexpr int kTw = kX;
-  static constexpr int kMod = kTw + tw_stage_total(N, E);  // N rows x C floats
+  static constexpr int kB = C * padk(N, pad_shift(E));  // >= N * C
+  static constexpr int kTw = 2 * kB;
+  static constexpr int kMod = kTw + tw_stage_total(N, E);
   static constexpr int kTotal = kMod + (N * C + 1) / 2;
 };
+
+// Synchronise the threads of one line when a line spans T > 32 threads
+// (whole warps): named barrier 1 + line, so lines do not wait for each other.
+template <int T>
+struct LineSync {
+  int id;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(T) : "memory");
+  }
+};
+
+// Does this step of the slot start with a row inverse FFT of G?
+__device__ __forceinline__ bool row_finishes(const Slot& s, int tick) {
+  const int step = tick - s.start_tick;
+  return step >= 1 && step <= s.n_iter;
+}
+
+// Copy the G rows of a row item into a buffer of padded strips.
+template <int N, int E>
+__device__ __forceinline__ void prefetch_row_tile(const Slot& s, int block, float2* buf) {
+  constexpr int L = lines_per_item(N, E);
+  constexpr int P = RowSmem<N, E>::kStrip;
+  cp_async_tile<L, N * 8, N * 8, P * 8>(buf, s.g + (size_t)block * L * N);
+}
 
 // ---------------------------------------------------------------------------
 // row pass for one item of a size-N slot
 //
-// The item's psi and support rows are requested with cp.async before the G
-// rows are loaded, so one memory latency is exposed per item and the update
-// reads them from shared memory.
+// On entry `gbuf` holds this item's G rows if `ready` (cp.async group pending,
+// the most recent one this thread committed); `pbuf` is free.  The psi and
+// support rows are requested at once and land while the inverse FFT runs.
+// After the update has consumed psi, the next item's G rows are requested
+// into `pbuf` (unless DM needs it as private storage); returns whether it
+// did, and the caller swaps the buffers.
 // ---------------------------------------------------------------------------
 template <int N, int E>
-__device__ __forceinline__ void row_item(const Slot& s, int step, int block, float2* smem,
+__device__ __forceinline__ bool row_item(const Slot& s, int step, int block, float2* gbuf,
+                                         float2* pbuf, bool ready, float* sup_tile,
+                                         const Slot* nxt, int nxt_block, int tick,
                                          const float2* __restrict__ tw) {
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
-  using Sync = typename std::conditional<(T <= 32), WarpSync, BlockSync>::type;
   constexpr int SH = pad_shift(E);
+  constexpr int P = RowSmem<N, E>::kStrip;
+  using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
   constexpr bool kFull = (L * T == kThreads);  // every thread owns a line segment
   const int tid = threadIdx.x;
   const int lrow = tid / T;
   const int t = tid - lrow * T;
   const bool active = kFull || lrow < L;
-  const int row = block * L + (active ? lrow : 0);
-  const RowLayout<SH> lay{smem + (active ? lrow : 0) * padk(N, SH)};
-  const Sync sync{};
+  const int lr = active ? lrow : 0;
+  const int row = block * L + lr;
+  const RowLayout<SH> lay{gbuf + lr * P};
+  Sync sync{};
+  if constexpr (T > 32) sync = Sync{1 + lr};
   const float b = s.beta;
   const size_t roff = (size_t)row * N + t;
-  const float2* __restrict__ g_in = s.g + roff;
   float2* psi = s.psi + roff;
+  const float2* gtile = gbuf + lr * P + t;    // this thread's G elements (unpadded row)
+  float2* psi_s = pbuf + lr * P + t;           // this thread's psi elements
+  const float* sup_s = sup_tile + lr * (N + 16) + t;
 
   bool finish, start;
   int alg_f, alg_s;
@@ -212,24 +263,36 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
     start = step < s.n_iter;
     alg_s = start ? slot_alg(s, step + 1) : SP_ER;
   }
+  // the next item's G rows go into pbuf once psi has been read, unless DM
+  // keeps private values there
+  const bool can_prefetch = nxt != nullptr && row_finishes(*nxt, tick) && alg_f != SP_DM && alg_s != SP_DM;
+  bool prefetched = false;
+  auto prefetch_next = [&]() {
+    if (can_prefetch) {
+      __syncthreads();  // every thread is done with pbuf
+      prefetch_row_tile<N, E>(*nxt, nxt_block, pbuf);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      prefetched = true;
+    }
+  };
 
-  using SM = RowSmem<N, E>;
-  // each thread only touches its own entries of the psi tile, so after the
-  // update has read psi_in the tile doubles as private storage for DM
-  float2* psi_s = smem + SM::kPsi + (active ? lrow : 0) * N + t;
-  const float* sup_s = reinterpret_cast<const float*>(smem + SM::kSup) +
-                       (active ? lrow : 0) * SM::kSupPitch + t;
   float2 v[E];
   if (finish) {
     const UpdateCoef cf = update_coef(alg_f, b);
-    // psi (when the update reads it) and support rows -> shared memory
     const size_t row0 = (size_t)block * L * N;
-    if (cf.needs_pi)
-      cp_async_rows(smem + SM::kPsi, s.psi + row0, 1, L * N * 8, 0, 0);
-    cp_async_rows(smem + SM::kSup, s.support + row0, L, N * 4, (size_t)N * 4, SM::kSupPitch * 4);
-    if (active) {
+    if (cf.needs_pi) cp_async_tile<L, N * 8, N * 8, P * 8>(pbuf, s.psi + row0);
+    cp_async_tile<L, N * 4, N * 4, (N + 16) * 4>(sup_tile, s.support + row0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    if (ready) {
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's G rows
+      __syncthreads();
+      if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = ld_stream(g_in + i * T);
+        for (int i = 0; i < E; ++i) v[i] = gtile[i * T];
+      }
+    } else if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + roff + i * T);
     }
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out
     cp_async_wait_all();
@@ -275,10 +338,11 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
         }
       }
     }
+    prefetch_next();
   } else {
     if (alg_s == SP_DM) {
-      cp_async_rows(smem + SM::kSup, s.support + (size_t)block * L * N, L, N * 4, (size_t)N * 4,
-                    SM::kSupPitch * 4);
+      cp_async_tile<L, N * 4, N * 4, (N + 16) * 4>(sup_tile, s.support + (size_t)block * L * N);
+      asm volatile("cp.async.commit_group;" ::: "memory");
     }
     if (active) {
 #pragma unroll
@@ -287,6 +351,8 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
     if (alg_s == SP_DM) {
       cp_async_wait_all();
       __syncthreads();
+    } else {
+      prefetch_next();
     }
   }
   if (start) {
@@ -315,6 +381,7 @@ __device__ __forceinline__ void row_item(const Slot& s, int step, int block, flo
       }
     }
   }
+  return prefetched;
 }
 
 // ---------------------------------------------------------------------------
@@ -348,7 +415,51 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
 }
 
 template <int N, int E>
-__device__ __forceinline__ void col_item(const Slot& s, int step, int block, float2* smem,
+__device__ __forceinline__ void cp_async_wait_group(int n) {
+  if (n >= 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Copy the G tile of a column item (N rows x C complex, row pitch C) into buf.
+template <int N, int E>
+__device__ __forceinline__ void prefetch_col_tile(const Slot& s, int block, float2* buf) {
+  constexpr int C = lines_per_item(N, E);
+  constexpr int RB = C * 8;
+  const float2* src = s.g + (size_t)block * C;
+  if constexpr (RB % 16 == 0) {
+    cp_async_tile<N, RB, N * 8, RB>(buf, src);
+  } else {
+    for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(buf + q * C, src + (size_t)q * N);
+  }
+}
+
+// Copy the modulus tile of a column item (N rows x C floats, row pitch C).
+template <int N, int E>
+__device__ __forceinline__ void stage_col_modulus(const Slot& s, int block, float* dst) {
+  constexpr int C = lines_per_item(N, E);
+  constexpr int RB = C * 4;
+  const float* src = s.modulus + (size_t)block * C;
+  if constexpr (RB % 16 == 0) {
+    cp_async_tile<N, RB, N * 4, RB>(dst, src);
+  } else {
+    for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(dst + q * C, src + (size_t)q * N);
+  }
+}
+
+// Does this step of the slot run a projection (and so want its G tile)?
+__device__ __forceinline__ bool col_projects(const Slot& s, int tick) {
+  const int step = tick - s.start_tick;
+  return step >= 1 && step <= s.n_iter;
+}
+
+// One column item.  On entry the cp.async groups pending for this thread are,
+// oldest first: this item's G tile (if `ready`), this item's modulus tile,
+// the next item's G tile.  `buf` holds this item's G tile (row pitch C) and
+// is then reused as the exchange buffer.
+template <int N, int E>
+__device__ __forceinline__ void col_item(const Slot& s, int step, int block, float2* buf,
+                                         bool ready, const float* mod_tile,
                                          const float2* __restrict__ tw, double* red) {
   constexpr int T = N / E;
   constexpr int C = lines_per_item(N, E);
@@ -359,28 +470,15 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   const int t = tid / C;
   const bool active = kFull || t < T;
   const int col = block * C + c;
-  const ColLayout<pad_shift(E), C> lay{smem + c};
+  const ColLayout<pad_shift(E), C> lay{buf + c};
   const BlockSync sync{};
   const size_t coff = (size_t)(active ? t : 0) * N + col;  // element (t + i*T, col) at coff + i*T*N
+  const float* mod_s = mod_tile + (active ? t : 0) * C + c;
 
-  using SM = ColSmem<N, E>;
-  const float* mod_s = reinterpret_cast<const float*>(smem + SM::kMod) + (active ? t : 0) * C + c;
-  auto stage_modulus = [&]() {
-    // N rows x C floats of the modulus -> shared memory (row pitch C floats)
-    constexpr int RB = C * 4;
-    const float* src = s.modulus + (size_t)block * C;
-    float* dst = reinterpret_cast<float*>(smem + SM::kMod);
-    if constexpr (RB % 16 == 0) {
-      cp_async_rows(dst, src, N, RB, (size_t)N * 4, RB);
-    } else {
-      for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(dst + q * C, src + (size_t)q * N);
-    }
-  };
   float2 v[E];
   if (step == 0) {
-    if (s.init != SP_INIT_RANDOM_PHASE) return;  // uniform over the block
-    stage_modulus();
-    cp_async_wait_all();
+    // random-phase start (no G tile was prefetched for step 0)
+    cp_async_wait_group<N, E>(1);  // the modulus tile
     __syncthreads();
     if (active) {
 #pragma unroll
@@ -405,8 +503,15 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
   const bool dm = slot_alg(s, step) == SP_DM;
   const bool want_err = s.err != nullptr;
   double e2 = 0.0, e1 = 0.0;
-  stage_modulus();
-  if (active) {
+  if (ready) {
+    cp_async_wait_group<N, E>(2);  // this item's G tile
+    __syncthreads();
+    if (active) {
+      const float2* tile = buf + t * C + c;
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = tile[i * T * C];
+    }
+  } else if (active) {
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + coff + (size_t)i * T * N);
   }
@@ -418,7 +523,7 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
     }
     fft_line<N, E, -1>(v, lay, sync, active, t, tw);
     if (plane == 0) {
-      cp_async_wait_all();
+      cp_async_wait_group<N, E>(1);  // the modulus tile
       __syncthreads();
     }
     project_cols<N, E>(v, mod_s, T * C, active, e2, e1, want_err && plane == 0);

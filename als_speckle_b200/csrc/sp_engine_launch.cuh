@@ -39,46 +39,108 @@ constexpr int min_blocks_for(int E, bool row) {
 // Build this size's per-stage twiddle tables in shared memory (once per
 // persistent CTA); returns their address.
 template <int N, int E>
-__device__ __forceinline__ const float2* stage_twiddles(float2* smem, const float2* __restrict__ tw_all) {
-  float2* tw = smem + item_smem_elems(N, E);  // = RowSmem::kTw = ColSmem::kTw
+__device__ __forceinline__ const float2* stage_twiddles(float2* tw, const float2* __restrict__ tw_all) {
   build_stage_twiddles<N, E>(tw, tw_all + N);
   __syncthreads();
   return tw;
 }
 
+// Row pass: persistent CTAs walk their items; the next item's G rows are
+// requested as soon as the current item's psi rows have been consumed.
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_kernel(PassArgs a) {
+  using SM = RowSmem<N, E>;
   extern __shared__ float2 smem[];
-  __shared__ Slot s;
+  __shared__ Slot sl[2];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
-  const float2* tw = stage_twiddles<N, E>(smem, a.tw);
-  for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
-    const Item item = a.items[it];
-    __syncthreads();  // previous item is done with smem and s
-    load_slot(&s, &a.slots[item.slot]);
+  const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);
+  float* sup_tile = reinterpret_cast<float*>(smem + SM::kSup);
+  int it = blockIdx.x;
+  int par = 0;
+  bool ready = false;
+  if (it < a.n_items) {
+    load_slot(&sl[0], &a.slots[a.items[it].slot]);
     __syncthreads();
-    const int step = tick - s.start_tick;
-    if (step < 0 || step > s.n_iter) continue;
-    row_item<N, E>(s, step, item.block, smem, tw);
+    if (row_finishes(sl[0], tick)) {
+      prefetch_row_tile<N, E>(sl[0], a.items[it].block, smem);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      ready = true;
+    }
   }
+  for (; it < a.n_items; it += gridDim.x) {
+    const int nit = it + gridDim.x;
+    __syncthreads();  // the previous item is done with both buffers and its slot
+    if (nit < a.n_items) load_slot(&sl[par ^ 1], &a.slots[a.items[nit].slot]);
+    __syncthreads();
+    const Slot& s = sl[par];
+    const int step = tick - s.start_tick;
+    bool next_ready = false;
+    if (step >= 0 && step <= s.n_iter) {
+      next_ready = row_item<N, E>(s, step, a.items[it].block, smem + par * SM::kB,
+                                  smem + (par ^ 1) * SM::kB, ready, sup_tile,
+                                  nit < a.n_items ? &sl[par ^ 1] : nullptr,
+                                  nit < a.n_items ? a.items[nit].block : 0, tick, tw);
+    }
+    if (!next_ready) {
+      // nothing is in flight for the next item: it keeps its G rows where
+      // they are (global memory) and the buffers need not swap
+      cp_async_wait_all();
+      ready = false;
+      continue;
+    }
+    ready = true;
+    par ^= 1;
+  }
+  cp_async_wait_all();
 }
 
+// Column pass: persistent CTAs walk their items with a two-stage pipeline.
+// At the top of item i the CTA requests (cp.async) item i's modulus tile and
+// then item i+gridDim's G tile into the buffer item i-gridDim used, so the
+// G tile of every item after the first arrives while the previous one is
+// transformed.
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_kernel(PassArgs a) {
+  using SM = ColSmem<N, E>;
   extern __shared__ float2 smem[];
-  __shared__ Slot s;
+  __shared__ Slot sl[2];
   __shared__ double red[2 * kThreads / 32];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
-  const float2* tw = stage_twiddles<N, E>(smem, a.tw);
-  for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
-    const Item item = a.items[it];
+  const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);
+  float* mod_tile = reinterpret_cast<float*>(smem + SM::kMod);
+  int it = blockIdx.x;
+  int par = 0;
+  bool ready = false;
+  if (it < a.n_items) {
+    load_slot(&sl[0], &a.slots[a.items[it].slot]);
     __syncthreads();
-    load_slot(&s, &a.slots[item.slot]);
-    __syncthreads();
-    const int step = tick - s.start_tick;
-    if (step < 0 || step > s.n_iter) continue;
-    col_item<N, E>(s, step, item.block, smem, tw, red);
+    if (col_projects(sl[0], tick)) {
+      prefetch_col_tile<N, E>(sl[0], a.items[it].block, smem);
+      ready = true;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  for (; it < a.n_items; it += gridDim.x) {
+    const int nit = it + gridDim.x;
+    __syncthreads();  // the previous item is done with its buffer, the modulus tile and its slot
+    if (nit < a.n_items) load_slot(&sl[par ^ 1], &a.slots[a.items[nit].slot]);
+    __syncthreads();
+    const Slot& s = sl[par];
+    const int step = tick - s.start_tick;
+    const bool live = step >= 0 && step <= s.n_iter && (step > 0 || s.init == SP_INIT_RANDOM_PHASE);
+    if (live) stage_col_modulus<N, E>(s, a.items[it].block, mod_tile);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    bool next_ready = false;
+    if (nit < a.n_items && col_projects(sl[par ^ 1], tick)) {
+      prefetch_col_tile<N, E>(sl[par ^ 1], a.items[nit].block, smem + (par ^ 1) * SM::kB);
+      next_ready = true;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    if (live) col_item<N, E>(s, step, a.items[it].block, smem + par * SM::kB, ready, mod_tile, tw, red);
+    ready = next_ready;
+    par ^= 1;
+  }
+  cp_async_wait_all();
 }
 
 template <int N, int E>
