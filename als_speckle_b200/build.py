@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libspeckle_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-ftz=true", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-I" + INCLUDE]
 
 
