@@ -139,23 +139,28 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Copy ROWS rows of RB bytes (a multiple of 16) starting at gsrc with global
 // row pitch GP bytes into shared memory with row pitch SP bytes, 16 bytes per
-// cp.async.  All geometry is compile-time, so each thread's chunk addresses
-// are a base plus constants.
-template <int ROWS, int RB, int GP, int SP>
-__device__ __forceinline__ void cp_async_tile(void* sdst, const void* gsrc) {
+// cp.async, shared among NT threads of which this is number q0.  All geometry
+// is compile-time, so each thread's chunk addresses are a base plus constants.
+template <int ROWS, int RB, int GP, int SP, int NT>
+__device__ __forceinline__ void cp_async_rows(void* sdst, const void* gsrc, int q0) {
   static_assert(RB % 16 == 0 && SP % 16 == 0 && GP % 16 == 0, "16-byte chunks");
   constexpr int PER_ROW = RB / 16;
   constexpr int CHUNKS = ROWS * PER_ROW;
   char* d = static_cast<char*>(sdst);
   const char* g = static_cast<const char*>(gsrc);
 #pragma unroll
-  for (int j = 0; j < (CHUNKS + kThreads - 1) / kThreads; ++j) {
-    const int q = threadIdx.x + j * kThreads;
-    if (CHUNKS % kThreads == 0 || q < CHUNKS) {
+  for (int j = 0; j < (CHUNKS + NT - 1) / NT; ++j) {
+    const int q = q0 + j * NT;
+    if (CHUNKS % NT == 0 || q < CHUNKS) {
       const int r = q / PER_ROW, c = q - r * PER_ROW;  // PER_ROW is a power of two
       cp_async<16>(d + r * SP + c * 16, g + (size_t)r * GP + c * 16);
     }
   }
+}
+// the same, shared by the whole block
+template <int ROWS, int RB, int GP, int SP>
+__device__ __forceinline__ void cp_async_tile(void* sdst, const void* gsrc) {
+  cp_async_rows<ROWS, RB, GP, SP, kThreads>(sdst, gsrc, threadIdx.x);
 }
 
 // Shared-memory plan of one pass item.  Row pass: exchange strips | twiddles |
@@ -199,56 +204,95 @@ struct LineSync {
   }
 };
 
+// Row-pass line groups.  The threads of a row item split into groups of
+// GT = max(T, 32) threads (a warp, or the warps of one line when T > 32);
+// group g owns lines [g*LPG, g*LPG + ROWS) of the item.  A group copies its
+// own rows (G, psi, support) and its own slot descriptor, so every wait in
+// the row pass is a warp or line barrier and the groups of a block run
+// independently of one another.
+template <int N, int E>
+struct RowGroup {
+  static constexpr int T = N / E;
+  static constexpr int L = lines_per_item(N, E);
+  static constexpr int GT = T < 32 ? 32 : T;
+  static constexpr int LPG = GT / T;
+  static constexpr int ROWS = LPG < L ? LPG : L;  // lines of every group that has any
+  static constexpr int NG = (L + LPG - 1) / LPG;  // groups with lines
+  static_assert(NG * GT <= kThreads && NG <= 15, "row groups");
+  using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
+  __device__ static Sync sync(int g) {
+    if constexpr (T <= 32) return Sync{};
+    else return Sync{1 + g};
+  }
+};
+
+// Copy one slot descriptor into shared memory, word by word, by the NT
+// threads of a group (q0 = thread index within it).
+template <int NT>
+__device__ __forceinline__ void load_slot_by(Slot* dst, const Slot* __restrict__ src, int q0) {
+  static_assert(sizeof(Slot) % 4 == 0, "slot size");
+  const int* sp = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(dst);
+#pragma unroll
+  for (int w = q0; w < (int)(sizeof(Slot) / 4); w += NT) d[w] = sp[w];
+}
+
 // Does this step of the slot start with a row inverse FFT of G?
 __device__ __forceinline__ bool row_finishes(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
   return step >= 1 && step <= s.n_iter;
 }
 
-// Copy the G rows of a row item into a buffer of padded strips.
+// Copy group g's G rows of a row item into its padded strips of buf.
 template <int N, int E>
-__device__ __forceinline__ void prefetch_row_tile(const Slot& s, int block, float2* buf) {
-  constexpr int L = lines_per_item(N, E);
+__device__ __forceinline__ void prefetch_row_tile(const Slot& s, int block, float2* buf, int g,
+                                                  int gtid) {
+  using RG = RowGroup<N, E>;
   constexpr int P = RowSmem<N, E>::kStrip;
-  cp_async_tile<L, N * 8, N * 8, P * 8>(buf, s.g + (size_t)block * L * N);
+  const int l0 = g * RG::LPG;
+  cp_async_rows<RG::ROWS, N * 8, N * 8, P * 8, RG::GT>(
+      buf + l0 * P, s.g + ((size_t)block * RG::L + l0) * N, gtid);
 }
 
 // ---------------------------------------------------------------------------
-// row pass for one item of a size-N slot
+// row pass for one item of a size-N slot, run by line group g (thread gtid of
+// it); `s` and `nxt` are the group's own copies of the slot descriptors.
 //
-// On entry `gbuf` holds this item's G rows if `ready` (cp.async group pending,
-// the most recent one this thread committed); `pbuf` is free.  The psi and
-// support rows are requested at once and land while the inverse FFT runs.
-// After the update has consumed psi, the next item's G rows are requested
-// into `pbuf` (unless DM needs it as private storage); returns whether it
-// did, and the caller swaps the buffers.
+// On entry `gbuf` holds the group's G rows of this item if `ready` (cp.async
+// group pending, the most recent one this thread committed); `pbuf` is free.
+// The psi and support rows are requested at once and land while the inverse
+// FFT runs.  After the update has consumed psi, the group's rows of the next
+// item's G are requested into `pbuf` (unless DM needs it as private
+// storage); returns whether it did, and the caller swaps the buffers.
 // ---------------------------------------------------------------------------
 template <int N, int E>
 __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, float2* gbuf,
                                          float2* pbuf, bool ready, float* sup_tile,
                                          const Slot* nxt, int nxt_block, int tick,
-                                         const float2* __restrict__ tw) {
+                                         const float2* __restrict__ tw, int g, int gtid) {
+  using RG = RowGroup<N, E>;
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
   constexpr int SH = pad_shift(E);
   constexpr int P = RowSmem<N, E>::kStrip;
-  using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
-  constexpr bool kFull = (L * T == kThreads);  // every thread owns a line segment
+  constexpr int SPITCH = RowSmem<N, E>::kSupPitch;
   const int tid = threadIdx.x;
+  constexpr bool kFull = (L * T == kThreads);  // every thread owns a line segment
   const int lrow = tid / T;
   const int t = tid - lrow * T;
   const bool active = kFull || lrow < L;
   const int lr = active ? lrow : 0;
   const int row = block * L + lr;
+  const int l0 = g * RG::LPG;  // the group's first line
   const RowLayout<SH> lay{gbuf + lr * P};
-  Sync sync{};
-  if constexpr (T > 32) sync = Sync{1 + lr};
+  const typename RG::Sync sync = RG::sync(g);
   const float b = s.beta;
   const size_t roff = (size_t)row * N + t;
+  const size_t grow0 = ((size_t)block * L + l0) * N;  // the group's first row in the plane
   float2* psi = s.psi + roff;
   const float2* gtile = gbuf + lr * P + t;    // this thread's G elements (unpadded row)
   float2* psi_s = pbuf + lr * P + t;           // this thread's psi elements
-  const float* sup_s = sup_tile + lr * (N + 16) + t;
+  const float* sup_s = sup_tile + lr * SPITCH + t;
 
   bool finish, start;
   int alg_f, alg_s;
@@ -269,23 +313,27 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
   bool prefetched = false;
   auto prefetch_next = [&]() {
     if (can_prefetch) {
-      __syncthreads();  // every thread is done with pbuf
-      prefetch_row_tile<N, E>(*nxt, nxt_block, pbuf);
+      sync();  // the group is done with its part of pbuf
+      prefetch_row_tile<N, E>(*nxt, nxt_block, pbuf, g, gtid);
       asm volatile("cp.async.commit_group;" ::: "memory");
       prefetched = true;
     }
+  };
+  auto copy_support = [&]() {
+    cp_async_rows<RG::ROWS, N * 4, N * 4, SPITCH * 4, RG::GT>(sup_tile + l0 * SPITCH,
+                                                              s.support + grow0, gtid);
   };
 
   float2 v[E];
   if (finish) {
     const UpdateCoef cf = update_coef(alg_f, b);
-    const size_t row0 = (size_t)block * L * N;
-    if (cf.needs_pi) cp_async_tile<L, N * 8, N * 8, P * 8>(pbuf, s.psi + row0);
-    cp_async_tile<L, N * 4, N * 4, (N + 16) * 4>(sup_tile, s.support + row0);
+    if (cf.needs_pi)
+      cp_async_rows<RG::ROWS, N * 8, N * 8, P * 8, RG::GT>(pbuf + l0 * P, s.psi + grow0, gtid);
+    copy_support();
     asm volatile("cp.async.commit_group;" ::: "memory");
     if (ready) {
       asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's G rows
-      __syncthreads();
+      sync();
       if (active) {
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = gtile[i * T];
@@ -296,7 +344,7 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
     }
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out
     cp_async_wait_all();
-    __syncthreads();
+    sync();
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -341,7 +389,7 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
     prefetch_next();
   } else {
     if (alg_s == SP_DM) {
-      cp_async_tile<L, N * 4, N * 4, (N + 16) * 4>(sup_tile, s.support + (size_t)block * L * N);
+      copy_support();
       asm volatile("cp.async.commit_group;" ::: "memory");
     }
     if (active) {
@@ -350,7 +398,7 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
     }
     if (alg_s == SP_DM) {
       cp_async_wait_all();
-      __syncthreads();
+      sync();
     } else {
       prefetch_next();
     }

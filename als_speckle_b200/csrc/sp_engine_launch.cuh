@@ -45,41 +45,49 @@ __device__ __forceinline__ const float2* stage_twiddles(float2* tw, const float2
   return tw;
 }
 
-// Row pass: persistent CTAs walk their items; the next item's G rows are
-// requested as soon as the current item's psi rows have been consumed.
+// Row pass: persistent CTAs walk their items; within a CTA each line group
+// (RowGroup) walks them on its own, with its own copies of the slot
+// descriptors and its own rows of every buffer, so no step of the loop waits
+// for the whole block.  The group's rows of the next item's G are requested
+// as soon as its psi rows of the current item have been consumed.
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_kernel(PassArgs a) {
   using SM = RowSmem<N, E>;
+  using RG = RowGroup<N, E>;
   extern __shared__ float2 smem[];
-  __shared__ Slot sl[2];
+  __shared__ Slot sl[2][RG::NG];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
-  const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);
+  const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);  // block barrier
   float* sup_tile = reinterpret_cast<float*>(smem + SM::kSup);
+  const int g = threadIdx.x / RG::GT;
+  const int gtid = threadIdx.x - g * RG::GT;
+  if (g >= RG::NG) return;  // no lines for this group (small N)
+  const auto sync = RG::sync(g);
   int it = blockIdx.x;
   int par = 0;
   bool ready = false;
   if (it < a.n_items) {
-    load_slot(&sl[0], &a.slots[a.items[it].slot]);
-    __syncthreads();
-    if (row_finishes(sl[0], tick)) {
-      prefetch_row_tile<N, E>(sl[0], a.items[it].block, smem);
+    load_slot_by<RG::GT>(&sl[0][g], &a.slots[a.items[it].slot], gtid);
+    sync();
+    if (row_finishes(sl[0][g], tick)) {
+      prefetch_row_tile<N, E>(sl[0][g], a.items[it].block, smem, g, gtid);
       asm volatile("cp.async.commit_group;" ::: "memory");
       ready = true;
     }
   }
   for (; it < a.n_items; it += gridDim.x) {
     const int nit = it + gridDim.x;
-    __syncthreads();  // the previous item is done with both buffers and its slot
-    if (nit < a.n_items) load_slot(&sl[par ^ 1], &a.slots[a.items[nit].slot]);
-    __syncthreads();
-    const Slot& s = sl[par];
+    sync();  // the group is done with its rows of both buffers and its slot copy
+    if (nit < a.n_items) load_slot_by<RG::GT>(&sl[par ^ 1][g], &a.slots[a.items[nit].slot], gtid);
+    sync();
+    const Slot& s = sl[par][g];
     const int step = tick - s.start_tick;
     bool next_ready = false;
     if (step >= 0 && step <= s.n_iter) {
       next_ready = row_item<N, E>(s, step, a.items[it].block, smem + par * SM::kB,
                                   smem + (par ^ 1) * SM::kB, ready, sup_tile,
-                                  nit < a.n_items ? &sl[par ^ 1] : nullptr,
-                                  nit < a.n_items ? a.items[nit].block : 0, tick, tw);
+                                  nit < a.n_items ? &sl[par ^ 1][g] : nullptr,
+                                  nit < a.n_items ? a.items[nit].block : 0, tick, tw, g, gtid);
     }
     if (!next_ready) {
       // nothing is in flight for the next item: it keeps its G rows where

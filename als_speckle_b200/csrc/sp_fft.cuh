@@ -61,8 +61,27 @@ __host__ __device__ constexpr double sin_frac(int k, int R) {
   return cos_frac(4 * k - R, 4 * R);  // sin(x) = cos(x - pi/2)
 }
 
-__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add and subtract as one packed FP32x2 instruction each (sm_100:
+// add/sub.f32x2 work on a 64-bit register pair, both lanes IEEE round to
+// nearest, flushed like the scalar code built with -ftz).  The butterflies are
+// almost all complex adds, so this halves their instruction count; products
+// stay scalar, where a packed form would need lane broadcasts or swaps.
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 ra, rb, rr;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.ftz.f32x2 rr, ra, rb;\n\tmov.b64 {%0, %1}, rr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 ra, rb, rr;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.ftz.f32x2 rr, ra, rb;\n\tmov.b64 {%0, %1}, rr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
 __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 w) {
@@ -92,9 +111,22 @@ __device__ __forceinline__ float2 twiddle_const(float2 a) {
 template <int R, int DIR, int K>
 __device__ __forceinline__ void dft_combine(float2* v, const float2* e, const float2* o) {
   if constexpr (K < R / 2) {
-    const float2 t = twiddle_const<R, DIR, K>(o[K]);
-    v[K] = e[K] + t;
-    v[K + R / 2] = e[K] - t;
+    if constexpr (4 * K == R) {
+      // twiddle -i (DIR < 0) or +i: a lane swap with a sign, folded into
+      // scalar adds (a packed add would first need the swapped pair)
+      const float2 a = e[K], b = o[K];
+      if constexpr (DIR < 0) {
+        v[K] = make_float2(a.x + b.y, a.y - b.x);
+        v[K + R / 2] = make_float2(a.x - b.y, a.y + b.x);
+      } else {
+        v[K] = make_float2(a.x - b.y, a.y + b.x);
+        v[K + R / 2] = make_float2(a.x + b.y, a.y - b.x);
+      }
+    } else {
+      const float2 t = twiddle_const<R, DIR, K>(o[K]);
+      v[K] = e[K] + t;
+      v[K + R / 2] = e[K] - t;
+    }
     dft_combine<R, DIR, K + 1>(v, e, o);
   }
 }

@@ -5,6 +5,9 @@
 // with, not part of the engine.
 #include <cufft.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "sp_common.cuh"
@@ -26,7 +29,6 @@ using namespace sp;
     cufftResult _r = (expr);                                                \
     if (_r != CUFFT_SUCCESS) {                                              \
       ::sp::set_error("%s failed: cufft status %d", #expr, (int)_r);        \
-      cufftDestroy(plan);                                                   \
       return SP_ERR_CUDA;                                                   \
     }                                                                       \
   } while (0)
@@ -37,10 +39,39 @@ using namespace sp;
     if (_e == cudaSuccess) _e = cudaStreamSynchronize(st);                  \
     if (_e != cudaSuccess) {                                                \
       ::sp::set_error("plain path: %s", cudaGetErrorString(_e));            \
-      cufftDestroy(plan);                                                   \
       return SP_ERR_CUDA;                                                   \
     }                                                                       \
   } while (0)
+
+namespace {
+// One cuFFT plan per (device, N), made on first use and kept, as the
+// reference makes its FFT plan once when the data are loaded
+// (phasing.py:1187-1230).  The lock is held for a whole call because the
+// plan's stream is set per call.
+std::mutex g_plan_mu;
+std::map<std::pair<int, int>, cufftHandle> g_plans;
+
+int plan_for(int N, cufftHandle* out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    ::sp::set_error("plain path: cudaGetDevice failed");
+    return SP_ERR_CUDA;
+  }
+  auto it = g_plans.find({dev, N});
+  if (it != g_plans.end()) {
+    *out = it->second;
+    return SP_OK;
+  }
+  cufftHandle plan = 0;
+  if (cufftPlan2d(&plan, N, N, CUFFT_C2C) != CUFFT_SUCCESS) {
+    ::sp::set_error("cufftPlan2d(%d) failed", N);
+    return SP_ERR_CUDA;
+  }
+  g_plans[{dev, N}] = plan;
+  *out = plan;
+  return SP_OK;
+}
+}  // namespace
 
 extern "C" int sp_plain_iterate(int N, int n_iter, int n_runs, const int32_t* run_alg,
                                 const int32_t* run_count, float beta, void* psi_dev,
@@ -65,19 +96,17 @@ extern "C" int sp_plain_iterate(int N, int n_iter, int n_runs, const int32_t* ru
   float2* fourier = psi_out + n;
   float2* div = fourier + n;
   float2* tmp = div + n;  // DM modified estimate / second projection
+  std::lock_guard<std::mutex> lock(g_plan_mu);
   cufftHandle plan = 0;
-  if (cufftPlan2d(&plan, N, N, CUFFT_C2C) != CUFFT_SUCCESS) {
-    set_error("cufftPlan2d(%d) failed", N);
-    return SP_ERR_CUDA;
-  }
+  if (int rc = plan_for(N, &plan); rc != SP_OK) return rc;
   SP_CUFFT_TRY(cufftSetStream(plan, st));
   const float inv = 1.0f / ((float)N * (float)N);
   auto project = [&](float2* in, float2* out) -> int {
     SP_CUFFT_TRY(cufftExecC2C(plan, (cufftComplex*)in, (cufftComplex*)fourier, CUFFT_FORWARD));
     SP_PLAIN_SYNC(st);
-    if (sp_abs_f2_f2(fourier, div, n, stream) != SP_OK) { cufftDestroy(plan); return SP_ERR_CUDA; }
+    if (sp_abs_f2_f2(fourier, div, n, stream) != SP_OK) return SP_ERR_CUDA;
     SP_PLAIN_SYNC(st);
-    if (sp_fourier(fourier, div, modulus_dev, fourier, n, stream) != SP_OK) { cufftDestroy(plan); return SP_ERR_CUDA; }
+    if (sp_fourier(fourier, div, modulus_dev, fourier, n, stream) != SP_OK) return SP_ERR_CUDA;
     SP_PLAIN_SYNC(st);
     SP_CUFFT_TRY(cufftExecC2C(plan, (cufftComplex*)fourier, (cufftComplex*)out, CUFFT_INVERSE));
     SP_PLAIN_SYNC(st);
@@ -109,12 +138,8 @@ extern "C" int sp_plain_iterate(int N, int n_iter, int n_runs, const int32_t* ru
         set_error("sp_plain_iterate: algorithm %d has no plain kernel", alg);
         break;
     }
-    if (rc != SP_OK) {
-      cufftDestroy(plan);
-      return rc;
-    }
+    if (rc != SP_OK) return rc;
     SP_PLAIN_SYNC(st);
   }
-  cufftDestroy(plan);
   return SP_OK;
 }
