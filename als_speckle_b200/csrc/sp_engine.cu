@@ -11,6 +11,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "sp_common.cuh"
@@ -135,6 +136,8 @@ static int validate(const sp_trial& t, int idx) {
 struct Layout {
   size_t slots_off, items_off, planes_off, total;
   std::vector<size_t> g_off, g2_off;
+  std::vector<size_t> mt_off;  // transposed modulus of each trial (shared by equal moduli)
+  std::vector<int> mt_first;   // trials that own a transposed modulus (first use)
   int n_items;
 };
 
@@ -165,8 +168,48 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
       off += align_up(plane);
     }
   }
+  // one transposed copy per distinct (modulus, N), for the column pass
+  std::map<std::pair<const float*, int>, size_t> seen;
+  L.mt_off.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const auto key = std::make_pair(trials[i].modulus_dev, trials[i].n);
+    auto f = seen.find(key);
+    if (f != seen.end()) {
+      L.mt_off[i] = f->second;
+      continue;
+    }
+    L.mt_off[i] = off;
+    seen[key] = off;
+    L.mt_first.push_back(i);
+    off += align_up((size_t)trials[i].n * trials[i].n * sizeof(float));
+  }
   L.total = off;
   return L;
+}
+
+// dst = src^T for an N x N float array (32 x 32 tiles through shared memory)
+__global__ void transpose_kernel(const float* __restrict__ src, float* __restrict__ dst, int N) {
+  __shared__ float tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y)
+    tile[y][threadIdx.x] = src[(size_t)(by + y) * N + bx + threadIdx.x];
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y)
+    dst[(size_t)(bx + y) * N + by + threadIdx.x] = tile[threadIdx.x][y];
+}
+
+// N = 8, 16: one block of N x N threads
+__global__ void transpose_small_kernel(const float* __restrict__ src, float* __restrict__ dst, int N) {
+  const int r = threadIdx.x / N, c = threadIdx.x % N;
+  dst[c * N + r] = src[r * N + c];
+}
+
+static cudaError_t launch_transpose(const float* src, float* dst, int N, cudaStream_t st) {
+  if (N >= 32)
+    transpose_kernel<<<dim3(N / 32, N / 32), dim3(32, 8), 0, st>>>(src, dst, N);
+  else
+    transpose_small_kernel<<<1, N * N, 0, st>>>(src, dst, N);
+  return cudaGetLastError();
 }
 
 // one launch target: the items of one size within one group
@@ -306,6 +349,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       s.g = reinterpret_cast<float2*>(ws + L.g_off[i]);
       s.g2 = L.g2_off[i] ? reinterpret_cast<float2*>(ws + L.g2_off[i]) : nullptr;
       s.modulus = t.modulus_dev;
+      s.modulus_t = reinterpret_cast<const float*>(ws + L.mt_off[i]);
       s.support = t.support_dev;
       s.save = static_cast<float2*>(t.save_dev);
       s.err = t.errors_dev;
@@ -323,10 +367,14 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       SP_CUDA_TRY(cudaMemsetAsync(trials[i].errors_dev, 0,
                                   sizeof(double) * 2 * (size_t)trials[i].n_iter, st));
   }
+  // the column pass reads each modulus transposed (rows of the copy are columns)
+  for (int i : L.mt_first)
+    SP_CUDA_TRY(launch_transpose(trials[i].modulus_dev, reinterpret_cast<float*>(ws + L.mt_off[i]),
+                                 trials[i].n, st));
   const Slot* dslots = reinterpret_cast<const Slot*>(ws + L.slots_off);
   const Item* ditems = reinterpret_cast<const Item*>(ws + L.items_off);
   const bool use_graph = opts && opts->use_graph && st != nullptr;
-  g_last_launches = 0;
+  g_last_launches = (int64_t)L.mt_first.size();
   for (int g = 0; g < n_groups; ++g) g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
 
   for (int g = 0; g < n_groups; ++g) {

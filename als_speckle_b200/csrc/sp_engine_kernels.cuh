@@ -34,6 +34,7 @@ struct Slot {
   float2* g;   // Fourier work plane
   float2* g2;  // second plane for DM (projection of dm1(psi)), or null
   const float* modulus;
+  const float* modulus_t;  // the modulus transposed (row c = column c), in the workspace
   const float* support;
   float2* save;
   double* err;
@@ -182,16 +183,47 @@ struct RowSmem {
   static constexpr int kSup = kTw + tw_stage_total(N, E);  // offset (float2 units)
   static constexpr int kTotal = kSup + (L * kSupPitch + 1) / 2;
 };
-// Column pass: two tile buffers (the G tile of the next item is copied into
-// one while the other holds the current item, first as its G tile, then as
-// its exchange buffer) | twiddles | modulus tile (N rows x C floats).
+// smallest y >= x with y = r (mod m)
+__host__ __device__ constexpr int next_congruent(int x, int r, int m) {
+  return x + ((r - x) % m + m) % m;
+}
+
+// Column-pass geometry.  An item is C adjacent columns; for its FFTs thread
+// tid works on column lc = tid / T at rows t + i*T (t = tid % T), so a column
+// belongs to half a warp, a warp, or a line group of T/32 warps, and the
+// exchanges of its transforms are warp (or line) synchronised.  Each column
+// has a strip of shared memory (element a at padk(a), pitch SP complex) for
+// its G values and exchanges, and a strip of its modulus (pitch MP floats),
+// copied by the column's own threads from the transposed modulus.
+//
+// The G tile crosses between the column layout and global rows in the
+// "row mapping" of the last Stockham stage: butterfly q = tid + u*256 of the
+// item is (row j = q / C, column c = q % C) and touches rows j + r*NSL,
+// r < RL, of column c (NSL, RL: the last stage's input stride and radix).  The
+// next item's G tile is copied in that mapping (8-byte cp.async), and the
+// last stage of the inverse transform runs in it one item later, straight
+// into global memory, so a copy overwrites only strip entries that the same
+// thread has just consumed.  With SP = 16/C (mod 16) for C <= 8 and SP odd
+// for C >= 16, every half-warp of those accesses touches 16 distinct 8-byte
+// bank pairs; MP staggers the modulus strips of columns that share a warp.
 template <int N, int E>
 struct ColSmem {
+  static constexpr int T = N / E;
   static constexpr int C = lines_per_item(N, E);
-  static constexpr int kB = C * padk(N, pad_shift(E));  // >= N * C
-  static constexpr int kTw = 2 * kB;
-  static constexpr int kMod = kTw + tw_stage_total(N, E);
-  static constexpr int kTotal = kMod + (N * C + 1) / 2;
+  static constexpr int SH = pad_shift(E);
+  static constexpr int SP = C >= 16 ? next_congruent(padk(N, SH), 1, 2)
+                                    : next_congruent(padk(N, SH), 16 / C, 16);
+  static constexpr int MP = T >= 32 ? N : N + (T >= 4 ? T : 4);
+  static constexpr int NSL = last_ns(N, E);      // last stage: inputs j + r*NSL
+  static constexpr int RL = N / NSL;             // last stage radix
+  static constexpr int BF = C * NSL;             // last-stage butterflies per item
+  static constexpr int kB = C * SP;              // float2 entries per G buffer
+  static constexpr int kTw = 2 * kB;             // offset of the twiddle tables
+  static constexpr int kMod = kTw + tw_stage_total(N, E);  // offset of the modulus strips
+  static constexpr int kTotal = kMod + (C * MP + 1) / 2;
+  // line groups for the modulus copy: GT threads own CG columns
+  static constexpr int GT = T < 32 ? 32 : T;
+  static constexpr int CG = (GT / T) < C ? (GT / T) : C;
 };
 
 // Synchronise the threads of one line when a line spans T > 32 threads
@@ -237,6 +269,15 @@ __device__ __forceinline__ void load_slot_by(Slot* dst, const Slot* __restrict__
   for (int w = q0; w < (int)(sizeof(Slot) / 4); w += NT) d[w] = sp[w];
 }
 
+// Request one slot descriptor into shared memory, 8 bytes per cp.async, by
+// the first threads of a group (q0 = thread index within it).
+__device__ __forceinline__ void copy_slot_by(Slot* dst, const Slot* src, int q0) {
+  static_assert(sizeof(Slot) % 8 == 0, "slot size");
+  constexpr int W = sizeof(Slot) / 8;
+  if (q0 < W)
+    cp_async<8>(reinterpret_cast<char*>(dst) + 8 * q0, reinterpret_cast<const char*>(src) + 8 * q0);
+}
+
 // Does this step of the slot start with a row inverse FFT of G?
 __device__ __forceinline__ bool row_finishes(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
@@ -263,13 +304,15 @@ __device__ __forceinline__ void prefetch_row_tile(const Slot& s, int block, floa
 // The psi and support rows are requested at once and land while the inverse
 // FFT runs.  After the update has consumed psi, the group's rows of the next
 // item's G are requested into `pbuf` (unless DM needs it as private
-// storage); returns whether it did, and the caller swaps the buffers.
+// storage); returns whether it did (with the caller's `extra` copies in the
+// same group), and the caller swaps the buffers.
 // ---------------------------------------------------------------------------
-template <int N, int E>
+template <int N, int E, class Extra>
 __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, float2* gbuf,
                                          float2* pbuf, bool ready, float* sup_tile,
                                          const Slot* nxt, int nxt_block, int tick,
-                                         const float2* __restrict__ tw, int g, int gtid) {
+                                         const float2* __restrict__ tw, int g, int gtid,
+                                         Extra&& extra) {
   using RG = RowGroup<N, E>;
   constexpr int T = N / E;
   constexpr int L = lines_per_item(N, E);
@@ -308,13 +351,15 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
     alg_s = start ? slot_alg(s, step + 1) : SP_ER;
   }
   // the next item's G rows go into pbuf once psi has been read, unless DM
-  // keeps private values there
-  const bool can_prefetch = nxt != nullptr && row_finishes(*nxt, tick) && alg_f != SP_DM && alg_s != SP_DM;
+  // keeps private values there; `extra` adds the caller's copies to that
+  // commit group.  (*nxt is read only here, after this item's first wait:
+  // its own copy may have travelled with this item's G rows.)
   bool prefetched = false;
   auto prefetch_next = [&]() {
-    if (can_prefetch) {
+    if (nxt != nullptr && alg_f != SP_DM && alg_s != SP_DM && row_finishes(*nxt, tick)) {
       sync();  // the group is done with its part of pbuf
       prefetch_row_tile<N, E>(*nxt, nxt_block, pbuf, g, gtid);
+      extra();
       asm volatile("cp.async.commit_group;" ::: "memory");
       prefetched = true;
     }
@@ -462,72 +507,155 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
   }
 }
 
-template <int N, int E>
-__device__ __forceinline__ void cp_async_wait_group(int n) {
-  if (n >= 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
-  else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
-  else asm volatile("cp.async.wait_group 0;" ::: "memory");
+// Is the slot live in the column pass at this tick (a projection, or the
+// random-phase start), and does it project (and so want its G tile)?
+__device__ __forceinline__ bool col_live(const Slot& s, int tick) {
+  const int step = tick - s.start_tick;
+  return step >= 0 && step <= s.n_iter && (step > 0 || s.init == SP_INIT_RANDOM_PHASE);
 }
-
-// Copy the G tile of a column item (N rows x C complex, row pitch C) into buf.
-template <int N, int E>
-__device__ __forceinline__ void prefetch_col_tile(const Slot& s, int block, float2* buf) {
-  constexpr int C = lines_per_item(N, E);
-  constexpr int RB = C * 8;
-  const float2* src = s.g + (size_t)block * C;
-  if constexpr (RB % 16 == 0) {
-    cp_async_tile<N, RB, N * 8, RB>(buf, src);
-  } else {
-    for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(buf + q * C, src + (size_t)q * N);
-  }
-}
-
-// Copy the modulus tile of a column item (N rows x C floats, row pitch C).
-template <int N, int E>
-__device__ __forceinline__ void stage_col_modulus(const Slot& s, int block, float* dst) {
-  constexpr int C = lines_per_item(N, E);
-  constexpr int RB = C * 4;
-  const float* src = s.modulus + (size_t)block * C;
-  if constexpr (RB % 16 == 0) {
-    cp_async_tile<N, RB, N * 4, RB>(dst, src);
-  } else {
-    for (int q = threadIdx.x; q < N; q += blockDim.x) cp_async<RB>(dst + q * C, src + (size_t)q * N);
-  }
-}
-
-// Does this step of the slot run a projection (and so want its G tile)?
 __device__ __forceinline__ bool col_projects(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
   return step >= 1 && step <= s.n_iter;
 }
 
-// One column item.  On entry the cp.async groups pending for this thread are,
-// oldest first: this item's G tile (if `ready`), this item's modulus tile,
-// the next item's G tile.  `buf` holds this item's G tile (row pitch C) and
-// is then reused as the exchange buffer.
+// This thread's last-stage butterflies of a column item: butterfly u is row
+// j(u) of column c, and pa(u, r) the strip offset of its row j(u) + r*NSL in
+// a G buffer.
 template <int N, int E>
-__device__ __forceinline__ void col_item(const Slot& s, int step, int block, float2* buf,
-                                         bool ready, const float* mod_tile,
-                                         const float2* __restrict__ tw, double* red) {
-  constexpr int T = N / E;
-  constexpr int C = lines_per_item(N, E);
+struct ColButterflies {
+  using CS = ColSmem<N, E>;
+  static constexpr int C = CS::C, SH = CS::SH, P = 1 << SH;
+  static constexpr int U = (CS::BF + kThreads - 1) / kThreads;
+  static constexpr int JS = kThreads / C;  // row step between a thread's butterflies
+  static constexpr bool LIN = (JS % P) == 0 && (CS::NSL % P) == 0;
+  int c, j0, pj0;
+  __device__ __forceinline__ ColButterflies()
+      : c(threadIdx.x % C), j0(threadIdx.x / C), pj0(c * CS::SP + padk(j0, SH)) {}
+  __device__ __forceinline__ bool valid(int u) const {
+    return CS::BF % kThreads == 0 || j0 + u * JS < CS::NSL;
+  }
+  __device__ __forceinline__ int j(int u) const { return j0 + u * JS; }
+  __device__ __forceinline__ int pa(int u, int r) const {
+    if constexpr (LIN) return pj0 + u * (JS + JS / P) + r * (CS::NSL + CS::NSL / P);
+    else return c * CS::SP + padk(j0 + u * JS + r * CS::NSL, SH);
+  }
+};
+
+// Request the G tile of a column item when it projects, in the row mapping.
+template <int N, int E>
+__device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, float2* gbuf) {
+  using CS = ColSmem<N, E>;
+  using BF = ColButterflies<N, E>;
+  if (!col_projects(s, tick)) return;
+  const BF bf;
+  const float2* g = s.g + block * CS::C + bf.c;
+#pragma unroll
+  for (int u = 0; u < BF::U; ++u) {
+    if (bf.valid(u)) {
+#pragma unroll
+      for (int r = 0; r < CS::RL; ++r)
+        cp_async<8>(gbuf + bf.pa(u, r), g + (size_t)(bf.j(u) + r * CS::NSL) * N);
+    }
+  }
+}
+
+// The last stage of the inverse column transforms of an item whose earlier
+// stages left their outputs in gbuf, run in the row mapping and written to
+// the plane g.  All inputs are read first; `then()` runs before the
+// arithmetic (the caller's next copies into gbuf go there: each overwrites
+// only entries this thread has already read).
+template <int N, int E, class Then>
+__device__ __forceinline__ void col_last_stage(float2* g, int block, const float2* gbuf,
+                                               const float2* __restrict__ tw, Then&& then) {
+  using CS = ColSmem<N, E>;
+  using BF = ColButterflies<N, E>;
+  constexpr int R = CS::RL, NS = CS::NSL;
+  const float2* __restrict__ tws = tw + tw_stage_offset(N, E, NS);
+  const BF bf;
+  float2 x[BF::U][R];
+#pragma unroll
+  for (int u = 0; u < BF::U; ++u) {
+    if (bf.valid(u)) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[u][r] = gbuf[bf.pa(u, r)];
+    }
+  }
+  then();
+  float2* dst = g + block * CS::C + bf.c;
+#pragma unroll
+  for (int u = 0; u < BF::U; ++u) {
+    if (bf.valid(u)) {
+      const int j = bf.j(u);
+#pragma unroll
+      for (int r = 1; r < R; ++r) x[u][r] = cmulc(x[u][r], tws[r * NS + j]);
+      dft<R, +1>(x[u]);
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst[(size_t)(j + r * NS) * N] = x[u][r];
+    }
+  }
+}
+
+// Each column's threads request their columns' modulus: rows of the
+// transposed modulus, 16 bytes per cp.async, into the columns' strips.
+template <int N, int E>
+__device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick, float* mod) {
+  using CS = ColSmem<N, E>;
+  if (!col_live(s, tick)) return;
+  const int g = threadIdx.x / CS::GT;
+  const int gtid = threadIdx.x - g * CS::GT;
+  const int lc0 = g * (CS::GT / CS::T);  // the group's first column
+  if (lc0 >= CS::C) return;
+  constexpr int PER_COL = N / 4;
+  constexpr int CHUNKS = CS::CG * PER_COL;
+  const float* src = s.modulus_t + (size_t)(block * CS::C + lc0) * N;
+  float* dst = mod + lc0 * CS::MP;
+#pragma unroll
+  for (int k = 0; k < (CHUNKS + CS::GT - 1) / CS::GT; ++k) {
+    const int q = gtid + k * CS::GT;
+    if (CHUNKS % CS::GT == 0 || q < CHUNKS) {
+      const int cc = q / PER_COL, off = (q - cc * PER_COL) * 4;
+      cp_async<16>(dst + cc * CS::MP + off, src + (size_t)cc * N + off);
+    }
+  }
+}
+
+// One column item, run by every thread of the block with no block-wide
+// barrier: each column's threads read their G elements from the column's
+// strip, transform, project with the modulus from the column's modulus strip
+// (the most recent cp.async group but one), and run the inverse transform up
+// to its last stage.  Returns the plane that col_last_stage must complete
+// (for DM the first plane is finished here and written directly, since the
+// second plane's transforms need the strips).
+template <int N, int E>
+__device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, float2* gbuf,
+                                            const float* mod, const float2* __restrict__ tw) {
+  using CS = ColSmem<N, E>;
+  constexpr int T = CS::T;
+  constexpr int C = CS::C;
+  constexpr int SH = CS::SH, P = 1 << SH;
   constexpr float inv = 1.0f / ((float)N * (float)N);
   constexpr bool kFull = (C * T == kThreads);
+  using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
   const int tid = threadIdx.x;
-  const int c = tid % C;
-  const int t = tid / C;
-  const bool active = kFull || t < T;
-  const int col = block * C + c;
-  const ColLayout<pad_shift(E), C> lay{buf + c};
-  const BlockSync sync{};
-  const size_t coff = (size_t)(active ? t : 0) * N + col;  // element (t + i*T, col) at coff + i*T*N
-  const float* mod_s = mod_tile + (active ? t : 0) * C + c;
+  const int lcol = tid / T;
+  const int t = tid - lcol * T;
+  const bool active = kFull || lcol < C;
+  const int lc = active ? lcol : 0;
+  const int col = block * C + lc;
+  const RowLayout<SH> lay{gbuf + lc * CS::SP};
+  Sync sync{};
+  if constexpr (T > 32) sync = Sync{1 + lc};
+  const size_t coff = (size_t)t * N + col;  // element (t + i*T, col) at coff + i*T*N
+  const float* mod_s = mod + lc * CS::MP + t;
+  auto wait_modulus = [&]() {
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    sync();
+  };
 
   float2 v[E];
   if (step == 0) {
-    // random-phase start (no G tile was prefetched for step 0)
-    cp_async_wait_group<N, E>(1);  // the modulus tile
-    __syncthreads();
+    // random-phase start: G = IFFT_cols(M exp(2 pi i u) / N^2)
+    wait_modulus();
     if (active) {
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -536,75 +664,57 @@ __device__ __forceinline__ void col_item(const Slot& s, int step, int block, flo
         const float u = (float)(h >> 8) * (1.0f / 16777216.0f);
         float sn, cs;
         sincospif(2.0f * u, &sn, &cs);
-        const float mm = mod_s[i * T * C] * inv;
+        const float mm = mod_s[i * T] * inv;
         v[i] = make_float2(mm * cs, mm * sn);
       }
     }
-    fft_line<N, E, +1>(v, lay, sync, active, t, tw);
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) s.g[coff + (size_t)i * T * N] = v[i];
-    }
-    return;
+    fft_line_head<N, E, +1>(v, lay, sync, active, t, tw);
+    return s.g;
   }
 
   const bool dm = slot_alg(s, step) == SP_DM;
   const bool want_err = s.err != nullptr;
   double e2 = 0.0, e1 = 0.0;
-  if (ready) {
-    cp_async_wait_group<N, E>(2);  // this item's G tile
-    __syncthreads();
-    if (active) {
-      const float2* tile = buf + t * C + c;
+  if (active) {
+    if constexpr (T % P == 0) {
+      const int p0 = padk(t, SH);
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = tile[i * T * C];
+      for (int i = 0; i < E; ++i) v[i] = lay.atp(p0 + i * (T + T / P));
+    } else {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
     }
-  } else if (active) {
-#pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + coff + (size_t)i * T * N);
   }
-  for (int plane = 0; plane < (dm ? 2 : 1); ++plane) {
-    float2* g = plane ? s.g2 : s.g;
-    if (plane && active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = ld_stream(g + coff + (size_t)i * T * N);
-    }
-    fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-    if (plane == 0) {
-      cp_async_wait_group<N, E>(1);  // the modulus tile
-      __syncthreads();
-    }
-    project_cols<N, E>(v, mod_s, T * C, active, e2, e1, want_err && plane == 0);
+  fft_line<N, E, -1>(v, lay, sync, active, t, tw);
+  wait_modulus();
+  project_cols<N, E>(v, mod_s, T, active, e2, e1, want_err);
+  float2* finish = s.g;
+  if (dm) {
     fft_line<N, E, +1>(v, lay, sync, active, t, tw);
     if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) g[coff + (size_t)i * T * N] = v[i];
+      for (int i = 0; i < E; ++i) s.g[coff + (size_t)i * T * N] = v[i];
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g2 + coff + (size_t)i * T * N);
     }
+    fft_line<N, E, -1>(v, lay, sync, active, t, tw);
+    project_cols<N, E>(v, mod_s, T, active, e2, e1, false);
+    finish = s.g2;
   }
+  fft_line_head<N, E, +1>(v, lay, sync, active, t, tw);
   if (want_err) {
-    // block reduction of the two FP64 partial sums, one atomic each per item
+    // warp sums of the FP64 partials, one atomic pair per warp
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       e2 += __shfl_xor_sync(0xffffffffu, e2, o);
       e1 += __shfl_xor_sync(0xffffffffu, e1, o);
     }
-    const int warp = tid >> 5;
-    __syncthreads();
     if ((tid & 31) == 0) {
-      red[2 * warp] = e2;
-      red[2 * warp + 1] = e1;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double a = 0.0, bsum = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) {
-        a += red[2 * w];
-        bsum += red[2 * w + 1];
-      }
-      atomicAdd(&s.err[2 * (step - 1)], a);
-      atomicAdd(&s.err[2 * (step - 1) + 1], bsum);
+      atomicAdd(&s.err[2 * (step - 1)], e2);
+      atomicAdd(&s.err[2 * (step - 1) + 1], e1);
     }
   }
+  return finish;
 }
 
 // shared-memory entries of one item's exchange buffer (rows: L padded strips;

@@ -23,6 +23,21 @@ __device__ __forceinline__ void load_slot(Slot* dst, const Slot* __restrict__ sr
   for (int w = threadIdx.x; w < (int)(sizeof(Slot) / 4); w += blockDim.x) d[w] = s[w];
 }
 
+// Request one slot descriptor into shared memory (8-byte cp.async by the
+// first threads of the block); it lands with the caller's next commit group.
+__device__ __forceinline__ void copy_slot(Slot* dst, const Slot* src) {
+  static_assert(sizeof(Slot) % 8 == 0, "slot size");
+  constexpr int W = sizeof(Slot) / 8;
+  if (threadIdx.x < W)
+    cp_async<8>(reinterpret_cast<char*>(dst) + 8 * threadIdx.x,
+                reinterpret_cast<const char*>(src) + 8 * threadIdx.x);
+}
+
+// An item read ahead into registers (slot < 0: none).
+__device__ __forceinline__ Item item_at(const PassArgs& a, int it) {
+  return it < a.n_items ? a.items[it] : Item{-1, 0};
+}
+
 // E = 32 keeps 64 registers of line data per thread plus the prefetched
 // psi/support: one 256-thread CTA per SM with up to 255 registers.  E = 16
 // halves that and runs two CTAs per SM.
@@ -46,108 +61,129 @@ __device__ __forceinline__ const float2* stage_twiddles(float2* tw, const float2
 }
 
 // Row pass: persistent CTAs walk their items; within a CTA each line group
-// (RowGroup) walks them on its own, with its own copies of the slot
-// descriptors and its own rows of every buffer, so no step of the loop waits
-// for the whole block.  The group's rows of the next item's G are requested
-// as soon as its psi rows of the current item have been consumed.
+// (RowGroup) walks them on its own, with its own ring of slot descriptors
+// (items k, k+1, k+2) and its own rows of every buffer, so no step of the
+// loop waits for the whole block.  The group's rows of the next item's G are
+// requested as soon as its psi rows of the current item have been consumed,
+// together with the descriptor of the item after that; the item list is read
+// ahead into registers.
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_kernel(PassArgs a) {
   using SM = RowSmem<N, E>;
   using RG = RowGroup<N, E>;
   extern __shared__ float2 smem[];
-  __shared__ Slot sl[2][RG::NG];
+  __shared__ __align__(16) Slot sl[3][RG::NG];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
   const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);  // block barrier
   float* sup_tile = reinterpret_cast<float*>(smem + SM::kSup);
   const int g = threadIdx.x / RG::GT;
   const int gtid = threadIdx.x - g * RG::GT;
-  if (g >= RG::NG) return;  // no lines for this group (small N)
-  const auto sync = RG::sync(g);
   int it = blockIdx.x;
-  int par = 0;
+  if (g >= RG::NG || it >= a.n_items) return;  // no lines for this group, or no items
+  const auto sync = RG::sync(g);
+  const int G = gridDim.x;
+  Item i0 = a.items[it], i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
+  load_slot_by<RG::GT>(&sl[0][g], &a.slots[i0.slot], gtid);
+  if (i1.slot >= 0) load_slot_by<RG::GT>(&sl[1][g], &a.slots[i1.slot], gtid);
+  sync();
   bool ready = false;
-  if (it < a.n_items) {
-    load_slot_by<RG::GT>(&sl[0][g], &a.slots[a.items[it].slot], gtid);
-    sync();
-    if (row_finishes(sl[0][g], tick)) {
-      prefetch_row_tile<N, E>(sl[0][g], a.items[it].block, smem, g, gtid);
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      ready = true;
-    }
+  if (row_finishes(sl[0][g], tick)) {
+    prefetch_row_tile<N, E>(sl[0][g], i0.block, smem, g, gtid);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    ready = true;
   }
-  for (; it < a.n_items; it += gridDim.x) {
-    const int nit = it + gridDim.x;
-    sync();  // the group is done with its rows of both buffers and its slot copy
-    if (nit < a.n_items) load_slot_by<RG::GT>(&sl[par ^ 1][g], &a.slots[a.items[nit].slot], gtid);
-    sync();
-    const Slot& s = sl[par][g];
+  int par = 0;
+  for (int k = 0; it < a.n_items; it += G, ++k) {
+    const Item i3 = item_at(a, it + 3 * G);
+    sync();  // the group is done with its rows of both buffers and with item k-1's slot entry
+    const Slot& s = sl[k % 3][g];
+    auto copy_ring = [&]() {  // item k+2's descriptor into item k-1's entry
+      if (i2.slot >= 0) copy_slot_by(&sl[(k + 2) % 3][g], &a.slots[i2.slot], gtid);
+    };
     const int step = tick - s.start_tick;
     bool next_ready = false;
     if (step >= 0 && step <= s.n_iter) {
-      next_ready = row_item<N, E>(s, step, a.items[it].block, smem + par * SM::kB,
-                                  smem + (par ^ 1) * SM::kB, ready, sup_tile,
-                                  nit < a.n_items ? &sl[par ^ 1][g] : nullptr,
-                                  nit < a.n_items ? a.items[nit].block : 0, tick, tw, g, gtid);
+      next_ready = row_item<N, E>(s, step, i0.block, smem + par * SM::kB, smem + (par ^ 1) * SM::kB,
+                                  ready, sup_tile, i1.slot >= 0 ? &sl[(k + 1) % 3][g] : nullptr,
+                                  i1.block, tick, tw, g, gtid, copy_ring);
     }
-    if (!next_ready) {
+    if (next_ready) {
+      ready = true;
+      par ^= 1;
+    } else {
       // nothing is in flight for the next item: it keeps its G rows where
       // they are (global memory) and the buffers need not swap
+      copy_ring();
+      asm volatile("cp.async.commit_group;" ::: "memory");
       cp_async_wait_all();
       ready = false;
-      continue;
     }
-    ready = true;
-    par ^= 1;
+    i0 = i1;
+    i1 = i2;
+    i2 = i3;
   }
   cp_async_wait_all();
 }
 
-// Column pass: persistent CTAs walk their items with a two-stage pipeline.
-// At the top of item i the CTA requests (cp.async) item i's modulus tile and
-// then item i+gridDim's G tile into the buffer item i-gridDim used, so the
-// G tile of every item after the first arrives while the previous one is
-// transformed.
+// Column pass: persistent CTAs walk their items with one block barrier per
+// item.  At the top of item k (after waiting for its G tile and the barrier)
+// the block reads the inputs of the last stage of item k-1's inverse
+// transforms from the other buffer, requests item k+1's G tile into that
+// buffer in the same mapping (each column's threads also request item k's
+// modulus), then finishes item k-1 straight into global memory; item k's
+// columns then run with no block-wide synchronisation.  Slot descriptors go
+// round a ring of three (items k, k+1 and k+2, whose copy is requested during
+// item k), and the item list is read ahead into registers, so no step of the
+// loop waits on a global load.
 template <int N, int E>
 __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_kernel(PassArgs a) {
-  using SM = ColSmem<N, E>;
+  using CS = ColSmem<N, E>;
   extern __shared__ float2 smem[];
-  __shared__ Slot sl[2];
-  __shared__ double red[2 * kThreads / 32];
+  __shared__ __align__(16) Slot sl[3];
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
-  const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);
-  float* mod_tile = reinterpret_cast<float*>(smem + SM::kMod);
+  const float2* tw = stage_twiddles<N, E>(smem + CS::kTw, a.tw);  // block barrier
+  float* mod = reinterpret_cast<float*>(smem + CS::kMod);
   int it = blockIdx.x;
-  int par = 0;
-  bool ready = false;
-  if (it < a.n_items) {
-    load_slot(&sl[0], &a.slots[a.items[it].slot]);
-    __syncthreads();
-    if (col_projects(sl[0], tick)) {
-      prefetch_col_tile<N, E>(sl[0], a.items[it].block, smem);
-      ready = true;
+  if (it >= a.n_items) return;  // the whole block leaves together
+  const int G = gridDim.x;
+  // items k, k+1, k+2 held in registers; item k+3 is read during item k
+  Item i0 = a.items[it], i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
+  load_slot(&sl[0], &a.slots[i0.slot]);
+  if (i1.slot >= 0) load_slot(&sl[1], &a.slots[i1.slot]);
+  __syncthreads();
+  copy_col_g<N, E>(sl[0], i0.block, tick, smem);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  float2* pend = nullptr;  // plane whose last stage is left in the other buffer
+  int pend_block = 0;
+  int b = 0;
+  for (int k = 0; it < a.n_items; it += G, ++k, b ^= 1) {
+    const Item i3 = item_at(a, it + 3 * G);
+    cp_async_wait_all();  // this item's G tile and item k+1's slot descriptor
+    __syncthreads();      // ... visible to all; the previous item is finished
+    float2* other = smem + (b ^ 1) * CS::kB;
+    const Slot& s = sl[k % 3];
+    auto copies = [&]() {
+      copy_col_mod<N, E>(s, i0.block, tick, mod);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      if (i1.slot >= 0) copy_col_g<N, E>(sl[(k + 1) % 3], i1.block, tick, other);
+      if (i2.slot >= 0) copy_slot(&sl[(k + 2) % 3], &a.slots[i2.slot]);  // item k-1's entry
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (pend)
+      col_last_stage<N, E>(pend, pend_block, other, tw, copies);
+    else
+      copies();
+    pend = nullptr;
+    if (col_live(s, tick)) {
+      pend = col_item<N, E>(s, tick - s.start_tick, i0.block, smem + b * CS::kB, mod, tw);
+      pend_block = i0.block;
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    i0 = i1;
+    i1 = i2;
+    i2 = i3;
   }
-  for (; it < a.n_items; it += gridDim.x) {
-    const int nit = it + gridDim.x;
-    __syncthreads();  // the previous item is done with its buffer, the modulus tile and its slot
-    if (nit < a.n_items) load_slot(&sl[par ^ 1], &a.slots[a.items[nit].slot]);
-    __syncthreads();
-    const Slot& s = sl[par];
-    const int step = tick - s.start_tick;
-    const bool live = step >= 0 && step <= s.n_iter && (step > 0 || s.init == SP_INIT_RANDOM_PHASE);
-    if (live) stage_col_modulus<N, E>(s, a.items[it].block, mod_tile);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    bool next_ready = false;
-    if (nit < a.n_items && col_projects(sl[par ^ 1], tick)) {
-      prefetch_col_tile<N, E>(sl[par ^ 1], a.items[nit].block, smem + (par ^ 1) * SM::kB);
-      next_ready = true;
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    if (live) col_item<N, E>(s, step, a.items[it].block, smem + par * SM::kB, ready, mod_tile, tw, red);
-    ready = next_ready;
-    par ^= 1;
-  }
+  __syncthreads();
+  if (pend) col_last_stage<N, E>(pend, pend_block, smem + (b ^ 1) * CS::kB, tw, [] {});
   cp_async_wait_all();
 }
 

@@ -226,14 +226,16 @@ struct BlockSync {
 };
 
 // Stages 2.. of the Stockham transform.  NS = product of radices done so far.
-template <int N, int E, int DIR, int NS, class Lay, class Sync>
+// HEAD stops before the last stage, whose inputs are then in shared memory.
+template <int N, int E, int DIR, int NS, bool HEAD, class Lay, class Sync>
 __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const Sync& sync,
                                            bool active, int t, const float2* __restrict__ tw) {
   constexpr int T = N / E;
   constexpr int SH = Lay::kShift;
   constexpr int P = 1 << SH;
-  if constexpr (NS < N) {
-    constexpr int R = (N / NS) < E ? (N / NS) : E;  // radix of this stage
+  constexpr int R_ = (N / NS) < E ? (N / NS) : E;
+  if constexpr (NS < N && !(HEAD && NS * R_ == N)) {
+    constexpr int R = R_;                           // radix of this stage
     constexpr int M = E / R;                        // butterflies per thread
     constexpr bool LAST = (NS * R == N);
     // element t + i*T: padded index padk(t) + i * TP when T is a multiple of P
@@ -294,7 +296,7 @@ __device__ __forceinline__ void fft_stages(float2 (&v)[E], const Lay& lay, const
     }
     if constexpr (!LAST) {
       sync();
-      fft_stages<N, E, DIR, NS * R, Lay, Sync>(v, lay, sync, active, t, tw);
+      fft_stages<N, E, DIR, NS * R, HEAD, Lay, Sync>(v, lay, sync, active, t, tw);
     }
   }
 }
@@ -326,7 +328,53 @@ __device__ __forceinline__ void fft_line(float2 (&v)[E], const Lay& lay, const S
       }
     }
     sync();
-    fft_stages<N, E, DIR, E, Lay, Sync>(v, lay, sync, active, t, tw);
+    fft_stages<N, E, DIR, E, false, Lay, Sync>(v, lay, sync, active, t, tw);
+  }
+}
+
+// Product of the radices before the last stage (N when the transform is the
+// single in-register stage, T = 1); the last stage has radix N / last_ns.
+__host__ __device__ constexpr int last_ns(int N, int E) {
+  int ns = E;
+  while (ns < N) {
+    const int r = (N / ns) < E ? (N / ns) : E;
+    if (ns * r == N) return ns;
+    ns *= r;
+  }
+  return N;
+}
+
+// fft_line without its last stage: on return the last stage's inputs are in
+// shared memory (Stockham index a at lay.at(a)), synchronised within the line;
+// with T = 1 the whole (in-register) transform is done and stored there.
+template <int N, int E, int DIR, class Lay, class Sync>
+__device__ __forceinline__ void fft_line_head(float2 (&v)[E], const Lay& lay, const Sync& sync,
+                                              bool active, int t, const float2* __restrict__ tw) {
+  static_assert(E <= N && (N % E) == 0, "E must divide N");
+  constexpr int T = N / E;
+  constexpr int SH = Lay::kShift;
+  dft<E, DIR>(v);
+  sync();  // previous readers of this shared buffer are done
+  if constexpr (T == 1) {
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) lay.at(r) = v[r];
+    }
+    sync();
+  } else {
+    constexpr bool LIN_WR = (E % (1 << SH)) == 0;
+    const int pw = padk(t * E, SH);
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        if constexpr (LIN_WR)
+          lay.atp(pw + r + (r >> SH)) = v[r];
+        else
+          lay.at(t * E + r) = v[r];
+      }
+    }
+    sync();
+    fft_stages<N, E, DIR, E, true, Lay, Sync>(v, lay, sync, active, t, tw);
   }
 }
 
