@@ -376,41 +376,48 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
       cp_async_rows<RG::ROWS, N * 8, N * 8, P * 8, RG::GT>(pbuf + l0 * P, s.psi + grow0, gtid);
     copy_support();
     asm volatile("cp.async.commit_group;" ::: "memory");
-    if (ready) {
-      asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's G rows
-      sync();
-      if (active) {
+    // one pass per plane (two for DM: G, then G2), so the transform is
+    // instantiated once
+    const int planes = alg_f == SP_DM ? 2 : 1;
+#pragma unroll 1
+    for (int plane = 0; plane < planes; ++plane) {
+      if (plane == 0) {
+        if (ready) {
+          asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's G rows
+          sync();
+          if (active) {
 #pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = gtile[i * T];
-      }
-    } else if (active) {
+            for (int i = 0; i < E; ++i) v[i] = gtile[i * T];
+          }
+        } else if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + roff + i * T);
-    }
-    fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out
-    cp_async_wait_all();
-    sync();
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const float sv = sup_s[i * T];
-        const float wa = cf.a0 + cf.a1 * sv;
-        const float wb = cf.b0 + cf.b1 * sv;
-        const float2 pi = cf.needs_pi ? psi_s[i * T] : make_float2(0.f, 0.f);
-        v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa + v[i].y * wb);
-      }
-    }
-    if (alg_f == SP_DM) {
-      // v holds the update without -s*b*t (parked in the psi tile);
-      // t = IFFT_rows(G2) is the second projection
-      if (active) {
-#pragma unroll
-        for (int i = 0; i < E; ++i) psi_s[i * T] = v[i];
+          for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g + roff + i * T);
+        }
+      } else if (active) {
+        // t = IFFT_rows(G2) is DM's second projection
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g2 + roff + i * T);
       }
-      fft_line<N, E, +1>(v, lay, sync, active, t, tw);
-      if (active) {
+      fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out (or t)
+      if (plane == 0) {
+        cp_async_wait_all();
+        sync();
+        if (active) {
+#pragma unroll
+          for (int i = 0; i < E; ++i) {
+            const float sv = sup_s[i * T];
+            const float wa = cf.a0 + cf.a1 * sv;
+            const float wb = cf.b0 + cf.b1 * sv;
+            const float2 pi = cf.needs_pi ? psi_s[i * T] : make_float2(0.f, 0.f);
+            v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa + v[i].y * wb);
+          }
+          // DM: the update without -s*b*t waits in the psi tile
+          if (planes == 2) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) psi_s[i * T] = v[i];
+          }
+        }
+      } else if (active) {
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           const float w = sup_s[i * T] * b;
@@ -449,7 +456,8 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
     }
   }
   if (start) {
-    if (alg_s == SP_DM && active) {
+    const int planes = alg_s == SP_DM ? 2 : 1;
+    if (planes == 2 && active) {
       // dm1(psi) waits in the psi tile while psi itself is transformed
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -457,20 +465,17 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
         psi_s[i * T] = make_float2(v[i].x * w, v[i].y * w);
       }
     }
-    fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) s.g[roff + i * T] = v[i];
-    }
-    if (alg_s == SP_DM) {
-      if (active) {
+#pragma unroll 1
+    for (int plane = 0; plane < planes; ++plane) {
+      if (plane == 1 && active) {
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = psi_s[i * T];
       }
       fft_line<N, E, -1>(v, lay, sync, active, t, tw);
+      float2* dst = (plane == 0 ? s.g : s.g2) + roff;
       if (active) {
 #pragma unroll
-        for (int i = 0; i < E; ++i) s.g2[roff + i * T] = v[i];
+        for (int i = 0; i < E; ++i) dst[i * T] = v[i];
       }
     }
   }
@@ -541,14 +546,13 @@ struct ColButterflies {
   }
 };
 
-// Request the G tile of a column item when it projects, in the row mapping.
+// Request the tile of a column item from the plane `plane`, in the row mapping.
 template <int N, int E>
-__device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, float2* gbuf) {
+__device__ __forceinline__ void copy_col_plane(const float2* plane, int block, float2* gbuf) {
   using CS = ColSmem<N, E>;
   using BF = ColButterflies<N, E>;
-  if (!col_projects(s, tick)) return;
   const BF bf;
-  const float2* g = s.g + block * CS::C + bf.c;
+  const float2* g = plane + block * CS::C + bf.c;
 #pragma unroll
   for (int u = 0; u < BF::U; ++u) {
     if (bf.valid(u)) {
@@ -557,6 +561,12 @@ __device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, f
         cp_async<8>(gbuf + bf.pa(u, r), g + (size_t)(bf.j(u) + r * CS::NSL) * N);
     }
   }
+}
+
+// Request the G tile of a column item when it projects.
+template <int N, int E>
+__device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, float2* gbuf) {
+  if (col_projects(s, tick)) copy_col_plane<N, E>(s.g, block, gbuf);
 }
 
 // The last stage of the inverse column transforms of an item whose earlier
@@ -624,8 +634,8 @@ __device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick,
 // strip, transform, project with the modulus from the column's modulus strip
 // (the most recent cp.async group but one), and run the inverse transform up
 // to its last stage.  Returns the plane that col_last_stage must complete
-// (for DM the first plane is finished here and written directly, since the
-// second plane's transforms need the strips).
+// (for DM the first plane is finished here and the second plane's tile
+// brought into the strips, which its transforms need).
 template <int N, int E>
 __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, float2* gbuf,
                                             const float* mod, const float2* __restrict__ tw) {
@@ -645,63 +655,66 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
   const RowLayout<SH> lay{gbuf + lc * CS::SP};
   Sync sync{};
   if constexpr (T > 32) sync = Sync{1 + lc};
-  const size_t coff = (size_t)t * N + col;  // element (t + i*T, col) at coff + i*T*N
   const float* mod_s = mod + lc * CS::MP + t;
   auto wait_modulus = [&]() {
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     sync();
   };
 
+  // One pass of the loop per plane (two for DM: G, then G2), so each
+  // transform is instantiated once.  A plane other than the last is finished
+  // here by the whole block, and the next plane's tile is brought into the
+  // strips through the same row-mapped copies as a prefetch.
+  const bool dm = step > 0 && slot_alg(s, step) == SP_DM;
+  const bool want_err = step > 0 && s.err != nullptr;
+  const int planes = dm ? 2 : 1;
+  double e2 = 0.0, e1 = 0.0;
   float2 v[E];
-  if (step == 0) {
-    // random-phase start: G = IFFT_cols(M exp(2 pi i u) / N^2)
-    wait_modulus();
-    if (active) {
+#pragma unroll 1
+  for (int plane = 0; plane < planes; ++plane) {
+    if (step == 0) {
+      // random-phase start: G = IFFT_cols(M exp(2 pi i u) / N^2)
+      wait_modulus();
+      if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const int k = t + i * T;
-        const uint32_t h = hash_u32(s.seed, s.trial, (uint32_t)(k * N + col));
-        const float u = (float)(h >> 8) * (1.0f / 16777216.0f);
-        float sn, cs;
-        sincospif(2.0f * u, &sn, &cs);
-        const float mm = mod_s[i * T] * inv;
-        v[i] = make_float2(mm * cs, mm * sn);
+        for (int i = 0; i < E; ++i) {
+          const int k = t + i * T;
+          const uint32_t h = hash_u32(s.seed, s.trial, (uint32_t)(k * N + col));
+          const float u = (float)(h >> 8) * (1.0f / 16777216.0f);
+          float sn, cs;
+          sincospif(2.0f * u, &sn, &cs);
+          const float mm = mod_s[i * T] * inv;
+          v[i] = make_float2(mm * cs, mm * sn);
+        }
       }
+    } else {
+      if (active) {  // the plane's tile, in the column's strip
+        if constexpr (T % P == 0) {
+          const int p0 = padk(t, SH);
+#pragma unroll
+          for (int i = 0; i < E; ++i) v[i] = lay.atp(p0 + i * (T + T / P));
+        } else {
+#pragma unroll
+          for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+        }
+      }
+      fft_line<N, E, -1>(v, lay, sync, active, t, tw);
+      if (plane == 0) wait_modulus();
+      project_cols<N, E>(v, mod_s, T, active, e2, e1, want_err && plane == 0);
     }
     fft_line_head<N, E, +1>(v, lay, sync, active, t, tw);
-    return s.g;
-  }
-
-  const bool dm = slot_alg(s, step) == SP_DM;
-  const bool want_err = s.err != nullptr;
-  double e2 = 0.0, e1 = 0.0;
-  if (active) {
-    if constexpr (T % P == 0) {
-      const int p0 = padk(t, SH);
-#pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = lay.atp(p0 + i * (T + T / P));
-    } else {
-#pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+    if (plane + 1 < planes) {
+      // finish G and bring in the G2 tile through the same strips (each
+      // thread's copies overwrite only entries it has already read)
+      __syncthreads();  // every column's last-stage inputs are in the strips
+      col_last_stage<N, E>(s.g, block, gbuf, tw, [&] {
+        copy_col_plane<N, E>(s.g2, block, gbuf);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      });
+      cp_async_wait_all();
+      __syncthreads();  // the G2 tile is in the strips
     }
   }
-  fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-  wait_modulus();
-  project_cols<N, E>(v, mod_s, T, active, e2, e1, want_err);
-  float2* finish = s.g;
-  if (dm) {
-    fft_line<N, E, +1>(v, lay, sync, active, t, tw);
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) s.g[coff + (size_t)i * T * N] = v[i];
-#pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g2 + coff + (size_t)i * T * N);
-    }
-    fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-    project_cols<N, E>(v, mod_s, T, active, e2, e1, false);
-    finish = s.g2;
-  }
-  fft_line_head<N, E, +1>(v, lay, sync, active, t, tw);
   if (want_err) {
     // warp sums of the FP64 partials, one atomic pair per warp
 #pragma unroll
@@ -714,7 +727,7 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
       atomicAdd(&s.err[2 * (step - 1) + 1], e1);
     }
   }
-  return finish;
+  return dm ? s.g2 : s.g;
 }
 
 // shared-memory entries of one item's exchange buffer (rows: L padded strips;
