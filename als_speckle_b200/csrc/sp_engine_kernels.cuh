@@ -8,9 +8,15 @@
 //   column pass  G <- IFFT_cols( P_M( FFT_cols(G) ) )   (+ FP64 error sums)
 //   row pass     psi_out = IFFT_rows(G); psi_in = update(...);
 //                G <- FFT_rows(psi_in)                   (start of next iteration)
+// Every transform runs in the forward direction: an inverse is done as
+// IFFT(x) = conj(FFT(conj(x))), with the conjugates folded into the
+// projection and the update, and G is stored conjugated between the column
+// pass and the row pass.  So each kernel holds one transform instance, which
+// keeps its code small.
 // Each pass is one persistent kernel over a work list of (slot, block) items;
 // a block is 256*E pixels of one trial (256*E/N rows, or 256*E/N columns),
-// where E (values per thread, 16 or 32) is chosen per size by the autotuner.  Which part of the schedule a slot is in
+// where E (values per thread, 16 or 32) is chosen per size by the autotuner.
+// Which part of the schedule a slot is in
 // comes from its own start tick, so trials of different sizes, algorithms and
 // iteration counts advance together in the same launches.
 #pragma once
@@ -370,17 +376,41 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
   };
 
   float2 v[E];
+  UpdateCoef cf{};
   if (finish) {
-    const UpdateCoef cf = update_coef(alg_f, b);
+    cf = update_coef(alg_f, b);
     if (cf.needs_pi)
       cp_async_rows<RG::ROWS, N * 8, N * 8, P * 8, RG::GT>(pbuf + l0 * P, s.psi + grow0, gtid);
     copy_support();
     asm volatile("cp.async.commit_group;" ::: "memory");
-    // one pass per plane (two for DM: G, then G2), so the transform is
-    // instantiated once
-    const int planes = alg_f == SP_DM ? 2 : 1;
+  } else {
+    if (alg_s == SP_DM) {
+      copy_support();
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = ld_stream(psi + i * T);
+    }
+    if (alg_s == SP_DM) {
+      cp_async_wait_all();
+      sync();
+    } else {
+      prefetch_next();
+    }
+  }
+  // Up to four transforms, one instance: finishing (G, and G2 for DM) and
+  // starting (psi, and dm1(psi) for DM).  The column pass leaves the work
+  // planes conjugated, so all of them run forward:
+  // IFFT_rows(G) = conj(FFT_rows(conj G)), the outer conjugate folded into
+  // the update.
+  const int nf = finish ? (alg_f == SP_DM ? 2 : 1) : 0;
+  const int nt = nf + (start ? (alg_s == SP_DM ? 2 : 1) : 0);
 #pragma unroll 1
-    for (int plane = 0; plane < planes; ++plane) {
+  for (int x = 0; x < nt; ++x) {
+    const bool fin = x < nf;
+    const int plane = fin ? x : x - nf;
+    if (fin) {
       if (plane == 0) {
         if (ready) {
           asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's G rows
@@ -398,8 +428,23 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = ld_stream(s.g2 + roff + i * T);
       }
-      fft_line<N, E, +1>(v, lay, sync, active, t, tw);  // v = psi_out (or t)
+    } else if (plane == 0) {
+      if (alg_s == SP_DM && active) {
+        // dm1(psi) waits in the psi tile while psi itself is transformed
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+          const float w = dm1_weight(b, sup_s[i * T]);
+          psi_s[i * T] = make_float2(v[i].x * w, v[i].y * w);
+        }
+      }
+    } else if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = psi_s[i * T];
+    }
+    fft_line<N, E, -1>(v, lay, sync, active, t, tw);
+    if (fin) {
       if (plane == 0) {
+        // psi_out = conj(v)
         cp_async_wait_all();
         sync();
         if (active) {
@@ -409,69 +454,39 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
             const float wa = cf.a0 + cf.a1 * sv;
             const float wb = cf.b0 + cf.b1 * sv;
             const float2 pi = cf.needs_pi ? psi_s[i * T] : make_float2(0.f, 0.f);
-            v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa + v[i].y * wb);
+            v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa - v[i].y * wb);
           }
           // DM: the update without -s*b*t waits in the psi tile
-          if (planes == 2) {
+          if (nf == 2) {
 #pragma unroll
             for (int i = 0; i < E; ++i) psi_s[i * T] = v[i];
           }
         }
       } else if (active) {
+        // t = conj(v)
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           const float w = sup_s[i * T] * b;
           const float2 p = psi_s[i * T];
-          v[i] = make_float2(p.x - w * v[i].x, p.y - w * v[i].y);
+          v[i] = make_float2(p.x - w * v[i].x, p.y + w * v[i].y);
         }
       }
-    }
-    if (active) {
+      if (plane == nf - 1) {
+        if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) psi[i * T] = v[i];
-      if (!start && s.save != nullptr && row >= s.r0 && row < s.r0 + s.rows) {
-        float2* dst = s.save + (size_t)(row - s.r0) * s.cols - s.c0;
+          for (int i = 0; i < E; ++i) psi[i * T] = v[i];
+          if (!start && s.save != nullptr && row >= s.r0 && row < s.r0 + s.rows) {
+            float2* dst = s.save + (size_t)(row - s.r0) * s.cols - s.c0;
 #pragma unroll
-        for (int i = 0; i < E; ++i) {
-          const int col = t + i * T;
-          if (col >= s.c0 && col < s.c0 + s.cols) dst[col] = v[i];
+            for (int i = 0; i < E; ++i) {
+              const int col = t + i * T;
+              if (col >= s.c0 && col < s.c0 + s.cols) dst[col] = v[i];
+            }
+          }
         }
+        prefetch_next();
       }
-    }
-    prefetch_next();
-  } else {
-    if (alg_s == SP_DM) {
-      copy_support();
-      asm volatile("cp.async.commit_group;" ::: "memory");
-    }
-    if (active) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = ld_stream(psi + i * T);
-    }
-    if (alg_s == SP_DM) {
-      cp_async_wait_all();
-      sync();
     } else {
-      prefetch_next();
-    }
-  }
-  if (start) {
-    const int planes = alg_s == SP_DM ? 2 : 1;
-    if (planes == 2 && active) {
-      // dm1(psi) waits in the psi tile while psi itself is transformed
-#pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const float w = dm1_weight(b, sup_s[i * T]);
-        psi_s[i * T] = make_float2(v[i].x * w, v[i].y * w);
-      }
-    }
-#pragma unroll 1
-    for (int plane = 0; plane < planes; ++plane) {
-      if (plane == 1 && active) {
-#pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = psi_s[i * T];
-      }
-      fft_line<N, E, -1>(v, lay, sync, active, t, tw);
       float2* dst = (plane == 0 ? s.g : s.g2) + roff;
       if (active) {
 #pragma unroll
@@ -485,7 +500,10 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
 // ---------------------------------------------------------------------------
 // column pass for one item of a size-N slot
 // ---------------------------------------------------------------------------
-// m_s[i * mstride] is the modulus of element i (shared memory)
+// m_s[i * mstride] is the modulus of element i (shared memory).  The result
+// is conjugated: the inverse column transform that follows runs as a
+// forward transform of the conjugate (IFFT(x) = conj(FFT(conj(x)))), so one
+// transform instance serves both directions.
 template <int N, int E>
 __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, int mstride,
                                              bool active, double& e2, double& e1, bool want_err) {
@@ -504,7 +522,7 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
     f1 += fabsf(d);
     // the reference divides by |F| = 0 (phasing_fourier.cl:14); keep M, zero phase
     const float sc = m[i] * rs * inv;
-    v[i] = p2 > 0.f ? make_float2(v[i].x * sc, v[i].y * sc) : make_float2(m[i] * inv, 0.f);
+    v[i] = p2 > 0.f ? make_float2(v[i].x * sc, v[i].y * -sc) : make_float2(m[i] * inv, 0.f);
   }
   if (want_err) {
     e2 += (double)f2;
@@ -570,8 +588,11 @@ __device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, f
 }
 
 // The last stage of the inverse column transforms of an item whose earlier
-// stages left their outputs in gbuf, run in the row mapping and written to
-// the plane g.  All inputs are read first; `then()` runs before the
+// stages left their (conjugated) outputs in gbuf, run in the row mapping as a
+// forward stage.  Its result, the conjugate of the new work plane, is
+// written to g as it is: the row pass transforms the conjugate (see
+// row_item), so the plane stays conjugated between the column pass and the
+// row pass.  All inputs are read first; `then()` runs before the
 // arithmetic (the caller's next copies into gbuf go there: each overwrites
 // only entries this thread has already read).
 template <int N, int E, class Then>
@@ -597,8 +618,8 @@ __device__ __forceinline__ void col_last_stage(float2* g, int block, const float
     if (bf.valid(u)) {
       const int j = bf.j(u);
 #pragma unroll
-      for (int r = 1; r < R; ++r) x[u][r] = cmulc(x[u][r], tws[r * NS + j]);
-      dft<R, +1>(x[u]);
+      for (int r = 1; r < R; ++r) x[u][r] = cmul(x[u][r], tws[r * NS + j]);
+      dft<R, -1>(x[u]);
 #pragma unroll
       for (int r = 0; r < R; ++r) dst[(size_t)(j + r * NS) * N] = x[u][r];
     }
@@ -673,10 +694,12 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
 #pragma unroll 1
   for (int plane = 0; plane < planes; ++plane) {
     if (step == 0) {
-      // random-phase start: G = IFFT_cols(M exp(2 pi i u) / N^2)
+      // random-phase start: G = IFFT_cols(M exp(2 pi i u) / N^2), written
+      // conjugated into the strip by a rolled loop (the hash and sincospif
+      // stay out of the unrolled code)
       wait_modulus();
       if (active) {
-#pragma unroll
+#pragma unroll 1
         for (int i = 0; i < E; ++i) {
           const int k = t + i * T;
           const uint32_t h = hash_u32(s.seed, s.trial, (uint32_t)(k * N + col));
@@ -684,25 +707,31 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
           float sn, cs;
           sincospif(2.0f * u, &sn, &cs);
           const float mm = mod_s[i * T] * inv;
-          v[i] = make_float2(mm * cs, mm * sn);
+          lay.at(k) = make_float2(mm * cs, -mm * sn);
         }
       }
-    } else {
-      if (active) {  // the plane's tile, in the column's strip
-        if constexpr (T % P == 0) {
-          const int p0 = padk(t, SH);
-#pragma unroll
-          for (int i = 0; i < E; ++i) v[i] = lay.atp(p0 + i * (T + T / P));
-        } else {
-#pragma unroll
-          for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
-        }
-      }
-      fft_line<N, E, -1>(v, lay, sync, active, t, tw);
-      if (plane == 0) wait_modulus();
-      project_cols<N, E>(v, mod_s, T, active, e2, e1, want_err && plane == 0);
     }
-    fft_line_head<N, E, +1>(v, lay, sync, active, t, tw);
+    if (active) {  // the plane's tile (or the start values), in the column's strip
+      if constexpr (T % P == 0) {
+        const int p0 = padk(t, SH);
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = lay.atp(p0 + i * (T + T / P));
+      } else {
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = lay.at(t + i * T);
+      }
+    }
+    // phase 0: forward transform and projection; phase 1: the inverse up to
+    // its last stage, as a forward transform of the conjugate
+#pragma unroll 1
+    for (int phase = step == 0 ? 1 : 0; phase < 2; ++phase) {
+      fft_line_head<N, E, -1>(v, lay, sync, active, t, tw);
+      if (phase == 0) {
+        fft_stages<N, E, -1, CS::NSL, false>(v, lay, sync, active, t, tw);  // its last stage
+        if (plane == 0) wait_modulus();
+        project_cols<N, E>(v, mod_s, T, active, e2, e1, want_err && plane == 0);
+      }
+    }
     if (plane + 1 < planes) {
       // finish G and bring in the G2 tile through the same strips (each
       // thread's copies overwrite only entries it has already read)
