@@ -235,7 +235,10 @@ static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, con
   for (int k = 0; k < n_ticks; ++k) {
     for (int which = 0; which < 2; ++which) {
       for (const Segment& sg : segs) {
-        PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw};
+        // the column pass walks the items backwards: it starts on the
+        // trials whose G planes the row pass wrote last (still in L2), and
+        // the next row pass starts on the ones it wrote last
+        PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw, which == 0 ? 1 : 0};
         SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid[which], st, a));
       }
     }

@@ -13,6 +13,7 @@ struct PassArgs {
   const int* tick_base;  // optional device counter added to tick_off
   int tick_off;
   const float2* tw;
+  int reverse;  // walk the item list from its end
 };
 
 // Copy one slot descriptor into shared memory (word by word).
@@ -35,7 +36,7 @@ __device__ __forceinline__ void copy_slot(Slot* dst, const Slot* src) {
 
 // An item read ahead into registers (slot < 0: none).
 __device__ __forceinline__ Item item_at(const PassArgs& a, int it) {
-  return it < a.n_items ? a.items[it] : Item{-1, 0};
+  return it < a.n_items ? a.items[a.reverse ? a.n_items - 1 - it : it] : Item{-1, 0};
 }
 
 // E = 32 keeps 64 registers of line data per thread plus the prefetched
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_ke
   if (g >= RG::NG || it >= a.n_items) return;  // no lines for this group, or no items
   const auto sync = RG::sync(g);
   const int G = gridDim.x;
-  Item i0 = a.items[it], i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
+  Item i0 = item_at(a, it), i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
   load_slot_by<RG::GT>(&sl[0][g], &a.slots[i0.slot], gtid);
   if (i1.slot >= 0) load_slot_by<RG::GT>(&sl[1][g], &a.slots[i1.slot], gtid);
   sync();
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
   if (it >= a.n_items) return;  // the whole block leaves together
   const int G = gridDim.x;
   // items k, k+1, k+2 held in registers; item k+3 is read during item k
-  Item i0 = a.items[it], i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
+  Item i0 = item_at(a, it), i1 = item_at(a, it + G), i2 = item_at(a, it + 2 * G);
   load_slot(&sl[0], &a.slots[i0.slot]);
   if (i1.slot >= 0) load_slot(&sl[1], &a.slots[i1.slot]);
   __syncthreads();
