@@ -154,11 +154,53 @@ def helpers():
     np.savez_compressed(os.path.join(HERE, "helpers.npz"), **out)
 
 
+def gaussian_ipsf(N, sigma):
+    """Transform of a normalised Gaussian point spread (sigma in pixels,
+    centred on pixel 0 with wrap-around): the ``ipsf`` that ``load`` takes."""
+    q = np.fft.fftfreq(N) * N
+    g = np.exp(-0.5 * (q[:, None] ** 2 + q[None, :] ** 2) / sigma ** 2)
+    g /= g.sum()
+    return np.fft.fft2(g).astype(np.complex64)
+
+
+def coherence():
+    """Partially coherent projections: one reference iteration of each
+    algorithm with ``load(ipsf=...)``, and a short trajectory."""
+    out = {}
+    for N in (32, 64):
+        psi, modulus, support = _inputs(N, 300 + N)
+        ipsf = gaussian_ipsf(N, 1.5)
+        out["N%d_psi" % N] = psi
+        out["N%d_modulus" % N] = modulus
+        out["N%d_support" % N] = support
+        out["N%d_ipsf" % N] = ipsf
+        for alg in ("hio", "er", "raar", "sf", "dm"):
+            beta = 0.9 if alg != "raar" else 0.87
+            r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+            _quiet(r.load, modulus=modulus, support=support, ipsf=ipsf, numtrials=1)
+            r.psi_in = psi.copy()
+            _quiet(r.iterate, 1, order=((alg, 1),), beta=beta)
+            out["N%d_%s_psi_in" % (N, alg)] = np.asarray(r.psi_in)
+            out["N%d_%s_beta" % (N, alg)] = np.float64(beta)
+    N = 32
+    psi, modulus, support = _inputs(N, 7)
+    ipsf = gaussian_ipsf(N, 1.0)
+    r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+    _quiet(r.load, modulus=modulus, support=support, ipsf=ipsf, numtrials=1)
+    r.psi_in = psi.copy()
+    _quiet(r.iterate, 8, order=(("hio", 3), ("dm", 2), ("er", 1)), beta=0.9)
+    out["traj_psi0"], out["traj_modulus"], out["traj_support"] = psi, modulus, support
+    out["traj_ipsf"] = ipsf
+    out["traj_psi_in"] = np.asarray(r.psi_in)
+    np.savez_compressed(os.path.join(HERE, "coherence.npz"), **out)
+
+
 if __name__ == "__main__":
     projections()
     trajectories()
     seeds()
     helpers()
+    coherence()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
