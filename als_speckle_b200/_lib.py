@@ -42,7 +42,7 @@ class sp_trial(C.Structure):
         ("beta", C.c_float), ("init", C.c_int32), ("seed", C.c_uint32), ("trial", C.c_uint32),
         ("r0", C.c_int32), ("c0", C.c_int32), ("rows", C.c_int32), ("cols", C.c_int32),
         ("psi_dev", C.c_void_p), ("modulus_dev", C.c_void_p), ("support_dev", C.c_void_p),
-        ("save_dev", C.c_void_p), ("errors_dev", C.c_void_p),
+        ("save_dev", C.c_void_p), ("errors_dev", C.c_void_p), ("ipsf_dev", C.c_void_p),
     ]
 
 

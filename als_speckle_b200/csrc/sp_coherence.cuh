@@ -1,0 +1,235 @@
+// Partially coherent projection (load(ipsf=...), phasing.py:1109-1137 and
+// :1187-1228): the modulus is replaced with the divisor
+//     div = sqrt(|IFFT2(FFT2(|F|^2) * ipsf)|),    F = FFT2(psi),
+// i.e. |F| blurred by the coherence function whose transform is ipsf.  The
+// divisor needs the whole 2-D |F|^2, so for these slots the engine's column
+// pass is replaced by three launches per projection plane (G, and G2 for DM):
+//   A (columns)  F = FFT_cols(G), stored over G;  W = FFT_cols(|F|^2)
+//   W (rows)     W = IFFT_rows(FFT_rows(W) * ipsf)           (unnormalised)
+//   B (columns)  div = sqrt(|IFFT_cols(W)|) / N;  P = M F / div;
+//                G = conj(IFFT_cols(P / N^2)) = FFT_cols(conj(P) / N^2)
+// B leaves G conjugated, as the engine's row pass expects.  The lines are
+// transformed with the engine's Stockham building blocks, E = min(16, N)
+// values per thread, one item (C columns or L rows of one plane) per block
+// iteration; work is a list of (slot, plane) jobs.
+#pragma once
+#include "sp_engine_kernels.cuh"
+
+namespace sp {
+
+struct PcArgs {
+  const Slot* slots;
+  const int2* jobs;  // (slot, plane)
+  int n_jobs;
+  int tick;
+  const float2* tw;  // twiddle table of all sizes
+};
+
+constexpr int pc_e(int N) { return N < 16 ? N : 16; }
+
+// Does job (slot, plane) project at this tick?
+__device__ __forceinline__ bool pc_active(const Slot& s, int plane, int tick) {
+  const int step = tick - s.start_tick;
+  return step >= 1 && step <= s.n_iter && (plane == 0 || slot_alg(s, step) == SP_DM);
+}
+
+template <int N>
+__host__ __device__ constexpr int pc_smem_elems() {
+  return item_smem_elems(N, pc_e(N)) + tw_stage_total(N, pc_e(N));
+}
+
+// A: F = FFT_cols(G) over G, W = FFT_cols(|F|^2).
+template <int N>
+__global__ void __launch_bounds__(kThreads) pc_cols_a_kernel(PcArgs a) {
+  constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
+  extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, a.tw + N);
+  const int tid = threadIdx.x, c = tid % C, t = tid / C;
+  const bool active = t < T;
+  const ColLayout<pad_shift(E), C> lay{smem + c};
+  constexpr int PER = N / C;
+  for (int it = blockIdx.x; it < a.n_jobs * PER; it += gridDim.x) {
+    const int j = it / PER, blk = it - j * PER;
+    const int2 job = a.jobs[j];
+    const Slot& s = a.slots[job.x];
+    if (!pc_active(s, job.y, a.tick)) continue;  // uniform over the block
+    float2* g = job.y ? s.g2 : s.g;
+    float2* w = job.y ? s.w2 : s.w;
+    const size_t off = (size_t)(active ? t : 0) * N + blk * C + c;
+    float2 v[E];
+    __syncthreads();  // the previous item's exchanges are done
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = g[off + (size_t)i * T * N];
+    }
+    fft_line<N, E, -1>(v, lay, BlockSync{}, active, t, tw);
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        g[off + (size_t)i * T * N] = v[i];
+        v[i] = make_float2(v[i].x * v[i].x + v[i].y * v[i].y, 0.f);
+      }
+    }
+    fft_line<N, E, -1>(v, lay, BlockSync{}, active, t, tw);
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) w[off + (size_t)i * T * N] = v[i];
+    }
+  }
+}
+
+// W: W = IFFT_rows(FFT_rows(W) * ipsf), unnormalised.
+template <int N>
+__global__ void __launch_bounds__(kThreads) pc_rows_w_kernel(PcArgs a) {
+  constexpr int E = pc_e(N), T = N / E, L = lines_per_item(N, E), SH = pad_shift(E);
+  using Sync = typename std::conditional<(T <= 32), WarpSync, BlockSync>::type;
+  extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, a.tw + N);
+  __syncthreads();
+  const int tid = threadIdx.x, lrow = tid / T, t = tid - lrow * T;
+  const bool active = lrow < L;
+  const int lr = active ? lrow : 0;
+  const RowLayout<SH> lay{smem + lr * padk(N, SH)};
+  constexpr int PER = N / L;
+  for (int it = blockIdx.x; it < a.n_jobs * PER; it += gridDim.x) {
+    const int j = it / PER, blk = it - j * PER;
+    const int2 job = a.jobs[j];
+    const Slot& s = a.slots[job.x];
+    if (!pc_active(s, job.y, a.tick)) continue;
+    float2* w = job.y ? s.w2 : s.w;
+    const size_t off = (size_t)(blk * L + lr) * N + t;
+    float2 v[E];
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = w[off + i * T];
+    }
+    fft_line<N, E, -1>(v, lay, Sync{}, active, t, tw);
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = cmul(v[i], s.ipsf[off + i * T]);
+    }
+    fft_line<N, E, +1>(v, lay, Sync{}, active, t, tw);
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) w[off + i * T] = v[i];
+    }
+  }
+}
+
+// B: divisor from W, projection of F (stored in G), inverse column transform;
+// FP64 error sums of |F| - M for plane 0, one atomic pair per warp.
+template <int N>
+__global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
+  constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
+  constexpr float inv = 1.0f / ((float)N * (float)N);
+  constexpr float inv_n = 1.0f / (float)N;
+  extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, a.tw + N);
+  const int tid = threadIdx.x, c = tid % C, t = tid / C;
+  const bool active = t < T;
+  const ColLayout<pad_shift(E), C> lay{smem + c};
+  constexpr int PER = N / C;
+  for (int it = blockIdx.x; it < a.n_jobs * PER; it += gridDim.x) {
+    const int j = it / PER, blk = it - j * PER;
+    const int2 job = a.jobs[j];
+    const Slot& s = a.slots[job.x];
+    if (!pc_active(s, job.y, a.tick)) continue;
+    const int step = a.tick - s.start_tick;
+    float2* g = job.y ? s.g2 : s.g;
+    const float2* w = job.y ? s.w2 : s.w;
+    const int col = blk * C + c;
+    const size_t off = (size_t)(active ? t : 0) * N + col;
+    float2 v[E];
+    float dv[E];
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = w[off + (size_t)i * T * N];
+    }
+    fft_line<N, E, +1>(v, lay, BlockSync{}, active, t, tw);
+    float f2 = 0.f, f1 = 0.f;
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) dv[i] = sqrtf(sqrtf(v[i].x * v[i].x + v[i].y * v[i].y)) * inv_n;
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const float2 f = g[off + (size_t)i * T * N];
+        const float m = s.modulus[off + (size_t)i * T * N];
+        const float d = sqrtf(f.x * f.x + f.y * f.y) - m;
+        f2 = fmaf(d, d, f2);
+        f1 += fabsf(d);
+        // the reference divides by a zero divisor; keep M with zero phase there
+        const float sc = dv[i] > 0.f ? m / dv[i] * inv : 0.f;
+        v[i] = dv[i] > 0.f ? make_float2(f.x * sc, f.y * -sc) : make_float2(m * inv, 0.f);
+      }
+    }
+    fft_line<N, E, -1>(v, lay, BlockSync{}, active, t, tw);  // = conj(IFFT_cols(P))
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) g[off + (size_t)i * T * N] = v[i];
+    }
+    if (job.y == 0 && s.err != nullptr) {
+      double e2 = f2, e1 = f1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+        e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+      }
+      if ((tid & 31) == 0) {
+        atomicAdd(&s.err[2 * (step - 1)], e2);
+        atomicAdd(&s.err[2 * (step - 1) + 1], e1);
+      }
+    }
+  }
+}
+
+// which: 0 = A, 1 = W, 2 = B
+template <int N>
+cudaError_t launch_pc_t(int which, int grid, cudaStream_t st, const PcArgs& a) {
+  const size_t sm = (size_t)pc_smem_elems<N>() * sizeof(float2);
+  if (which == 0) pc_cols_a_kernel<N><<<grid, kThreads, sm, st>>>(a);
+  else if (which == 1) pc_rows_w_kernel<N><<<grid, kThreads, sm, st>>>(a);
+  else pc_cols_b_kernel<N><<<grid, kThreads, sm, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t pc_setup_t() {
+  const int sm = pc_smem_elems<N>() * (int)sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(pc_cols_a_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(pc_rows_w_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(pc_cols_b_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+// work items per job (columns blocks = row blocks)
+template <int N>
+constexpr int pc_items_per_job() { return N / lines_per_item(N, pc_e(N)); }
+
+}  // namespace sp
+
+namespace sp {
+#define SP_DECLARE_PC(N)                                                              \
+  cudaError_t launch_pc_n##N(int which, int grid, cudaStream_t st, const PcArgs& a); \
+  cudaError_t pc_setup_n##N();
+SP_DECLARE_PC(8)
+SP_DECLARE_PC(16)
+SP_DECLARE_PC(32)
+SP_DECLARE_PC(64)
+SP_DECLARE_PC(128)
+SP_DECLARE_PC(256)
+SP_DECLARE_PC(512)
+SP_DECLARE_PC(1024)
+SP_DECLARE_PC(2048)
+SP_DECLARE_PC(4096)
+
+#define SP_DEFINE_PC(N)                                                                \
+  cudaError_t launch_pc_n##N(int which, int grid, cudaStream_t st, const PcArgs& a) { \
+    return launch_pc_t<N>(which, grid, st, a);                                        \
+  }                                                                                    \
+  cudaError_t pc_setup_n##N() { return pc_setup_t<N>(); }
+}  // namespace sp

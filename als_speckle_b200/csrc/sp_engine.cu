@@ -14,6 +14,7 @@
 #include <utility>
 #include <vector>
 
+#include "sp_coherence.cuh"
 #include "sp_common.cuh"
 #include "sp_engine_launch.cuh"
 
@@ -52,6 +53,38 @@ static cudaError_t pass_setup(int N, int E, int* occ) {
   }
 }
 
+static cudaError_t launch_pc(int N, int which, int grid, cudaStream_t st, const PcArgs& a) {
+  switch (N) {
+    case 8: return launch_pc_n8(which, grid, st, a);
+    case 16: return launch_pc_n16(which, grid, st, a);
+    case 32: return launch_pc_n32(which, grid, st, a);
+    case 64: return launch_pc_n64(which, grid, st, a);
+    case 128: return launch_pc_n128(which, grid, st, a);
+    case 256: return launch_pc_n256(which, grid, st, a);
+    case 512: return launch_pc_n512(which, grid, st, a);
+    case 1024: return launch_pc_n1024(which, grid, st, a);
+    case 2048: return launch_pc_n2048(which, grid, st, a);
+    case 4096: return launch_pc_n4096(which, grid, st, a);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static cudaError_t pc_setup_size(int N) {
+  switch (N) {
+    case 8: return pc_setup_n8();
+    case 16: return pc_setup_n16();
+    case 32: return pc_setup_n32();
+    case 64: return pc_setup_n64();
+    case 128: return pc_setup_n128();
+    case 256: return pc_setup_n256();
+    case 512: return pc_setup_n512();
+    case 1024: return pc_setup_n1024();
+    case 2048: return pc_setup_n2048();
+    case 4096: return pc_setup_n4096();
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // Per device, per (logN, E): dynamic-smem attributes set and the resident CTAs
 // per SM of the column pass ([0]) and row pass ([1]) cached.
 static std::mutex g_setup_mutex;
@@ -79,6 +112,22 @@ static cudaError_t occupancy_for(int N, int E, int* occ, int* sms) {
   occ[0] = g_occ[dev][l][k][0];
   occ[1] = g_occ[dev][l][k][1];
   *sms = g_sms[dev];
+  return cudaSuccess;
+}
+
+// Per device, per logN: the partial-coherence kernels' dynamic-smem attribute.
+static bool g_pc_ready[64][13];
+static cudaError_t pc_ready(int N) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_pc_ready[dev][ilog2(N)]) {
+    e = pc_setup_size(N);
+    if (e != cudaSuccess) return e;
+    g_pc_ready[dev][ilog2(N)] = true;
+  }
   return cudaSuccess;
 }
 
@@ -119,8 +168,9 @@ static int validate(const sp_trial& t, int idx) {
   SP_CHECK(period > 0, SP_ERR_INVALID, "trial %d: empty iteration order", idx);
   SP_CHECK(t.psi_dev && t.modulus_dev && t.support_dev, SP_ERR_INVALID,
            "trial %d: psi, modulus and support pointers are required", idx);
-  SP_CHECK(((uintptr_t)t.psi_dev | (uintptr_t)t.modulus_dev | (uintptr_t)t.support_dev) % 16 == 0,
-           SP_ERR_INVALID, "trial %d: psi, modulus and support must be 16-byte aligned", idx);
+  SP_CHECK(((uintptr_t)t.psi_dev | (uintptr_t)t.modulus_dev | (uintptr_t)t.support_dev |
+            (uintptr_t)t.ipsf_dev) % 16 == 0,
+           SP_ERR_INVALID, "trial %d: psi, modulus, support and ipsf must be 16-byte aligned", idx);
   SP_CHECK(t.init == SP_INIT_GIVEN || t.init == SP_INIT_RANDOM_PHASE, SP_ERR_INVALID,
            "trial %d: unknown init mode %d", idx, t.init);
   if (uses_dm(t)) SP_CHECK(t.beta != 0.f, SP_ERR_INVALID, "trial %d: DM needs beta != 0", idx);
@@ -138,7 +188,9 @@ struct Layout {
   std::vector<size_t> g_off, g2_off;
   std::vector<size_t> mt_off;  // transposed modulus of each trial (shared by equal moduli)
   std::vector<int> mt_first;   // trials that own a transposed modulus (first use)
-  int n_items;
+  std::vector<size_t> w_off, w2_off;  // partial-coherence divisor planes (0 = none)
+  size_t jobs_off;             // (slot, plane) jobs of the partial-coherence kernels
+  int n_items, n_jobs;
 };
 
 static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts) {
@@ -154,7 +206,12 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
     items += N / lines_per_item(N, effective_e(N, kMinE));
   }
   L.n_items = items;
-  L.planes_off = L.items_off + align_up(sizeof(Item) * (size_t)std::max(items, 1));
+  int jobs = 0;
+  for (int i = 0; i < n; ++i)
+    if (trials[i].ipsf_dev) jobs += uses_dm(trials[i]) ? 2 : 1;
+  L.n_jobs = jobs;
+  L.jobs_off = L.items_off + align_up(sizeof(Item) * (size_t)std::max(items, 1));
+  L.planes_off = L.jobs_off + align_up(sizeof(int2) * (size_t)std::max(jobs, 1));
   size_t off = L.planes_off;
   L.g_off.resize(n);
   L.g2_off.resize(n);
@@ -165,6 +222,19 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
     L.g2_off[i] = 0;
     if (uses_dm(trials[i])) {
       L.g2_off[i] = off;
+      off += align_up(plane);
+    }
+  }
+  // divisor planes of partially coherent trials, one per projection plane
+  L.w_off.assign(n, 0);
+  L.w2_off.assign(n, 0);
+  for (int i = 0; i < n; ++i) {
+    if (!trials[i].ipsf_dev) continue;
+    const size_t plane = (size_t)trials[i].n * trials[i].n * sizeof(float2);
+    L.w_off[i] = off;
+    off += align_up(plane);
+    if (uses_dm(trials[i])) {
+      L.w2_off[i] = off;
       off += align_up(plane);
     }
   }
@@ -215,6 +285,7 @@ static cudaError_t launch_transpose(const float* src, float* dst, int N, cudaStr
 // one launch target: the items of one size within one group
 struct Segment {
   int N, E, first, count, grid[2];  // grid[pass]: 0 column, 1 row
+  int pc_first, pc_count, pc_grid;  // partial-coherence jobs of this size
 };
 
 struct GraphKey {
@@ -231,8 +302,14 @@ static std::map<GraphKey, cudaGraphExec_t> g_graphs;
 static thread_local int64_t g_last_launches = 0;
 
 static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, const Item* items,
-                        int n_ticks, const float2* tw, cudaStream_t st) {
+                        const int2* jobs, int n_ticks, const float2* tw, cudaStream_t st) {
   for (int k = 0; k < n_ticks; ++k) {
+    // partially coherent projections first (their slots sit out the column pass)
+    for (const Segment& sg : segs) {
+      if (sg.pc_count == 0) continue;
+      PcArgs pa{slots, jobs + sg.pc_first, sg.pc_count, k, tw};
+      for (int which = 0; which < 3; ++which) SP_CUDA_TRY(launch_pc(sg.N, which, sg.pc_grid, st, pa));
+    }
     for (int which = 0; which < 2; ++which) {
       for (const Segment& sg : segs) {
         // the column pass walks the items backwards: it starts on the
@@ -300,6 +377,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
   std::vector<Slot> hs(n_trials);
   std::vector<Item> hi;
   hi.reserve(L.n_items);
+  std::vector<int2> hj;  // partial-coherence jobs (slot, plane)
+  hj.reserve(L.n_jobs);
   std::vector<std::vector<Segment>> segs(n_groups);
   std::vector<int> ticks(n_groups, 0);
   for (int g = 0; g < n_groups; ++g) {
@@ -315,11 +394,22 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       if (count == 0) continue;
       int occ[2] = {1, 1}, sms = 1;
       SP_CUDA_TRY(occupancy_for(N, E, occ, &sms));
-      Segment sg{N, E, first, count, {1, 1}};
+      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1};
       for (int p = 0; p < 2; ++p) {
         int per_sm = occ[p];
         if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
         sg.grid[p] = std::max(1, std::min(count, sms * per_sm));
+      }
+      for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
+        if (trials[i].n != N || !trials[i].ipsf_dev) continue;
+        hj.push_back(int2{i, 0});
+        if (uses_dm(trials[i])) hj.push_back(int2{i, 1});
+      }
+      sg.pc_count = (int)hj.size() - sg.pc_first;
+      if (sg.pc_count > 0) {
+        SP_CUDA_TRY(pc_ready(N));
+        const int per_job = N / lines_per_item(N, pc_e(N));
+        sg.pc_grid = std::max(1, std::min(sg.pc_count * per_job, sms * 4));
       }
       segs[g].push_back(sg);
     }
@@ -356,14 +446,22 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       s.support = t.support_dev;
       s.save = static_cast<float2*>(t.save_dev);
       s.err = t.errors_dev;
+      s.ipsf = static_cast<const float2*>(t.ipsf_dev);
+      s.w = L.w_off[i] ? reinterpret_cast<float2*>(ws + L.w_off[i]) : nullptr;
+      s.w2 = L.w2_off[i] ? reinterpret_cast<float2*>(ws + L.w2_off[i]) : nullptr;
     }
   }
   SP_CHECK((int)hi.size() <= L.n_items, SP_ERR_INVALID,
            "internal: %zu work items exceed the %d reserved", hi.size(), L.n_items);
+  SP_CHECK((int)hj.size() == L.n_jobs, SP_ERR_INVALID,
+           "internal: %zu partial-coherence jobs, %d reserved", hj.size(), L.n_jobs);
   SP_CUDA_TRY(cudaMemcpyAsync(ws + L.slots_off, hs.data(), sizeof(Slot) * hs.size(),
                               cudaMemcpyHostToDevice, st));
   if (!hi.empty())
     SP_CUDA_TRY(cudaMemcpyAsync(ws + L.items_off, hi.data(), sizeof(Item) * hi.size(),
+                                cudaMemcpyHostToDevice, st));
+  if (!hj.empty())
+    SP_CUDA_TRY(cudaMemcpyAsync(ws + L.jobs_off, hj.data(), sizeof(int2) * hj.size(),
                                 cudaMemcpyHostToDevice, st));
   for (int i = 0; i < n_trials; ++i) {
     if (trials[i].errors_dev && trials[i].n_iter > 0)
@@ -376,19 +474,25 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
                                  trials[i].n, st));
   const Slot* dslots = reinterpret_cast<const Slot*>(ws + L.slots_off);
   const Item* ditems = reinterpret_cast<const Item*>(ws + L.items_off);
+  const int2* djobs = reinterpret_cast<const int2*>(ws + L.jobs_off);
   const bool use_graph = opts && opts->use_graph && st != nullptr;
   g_last_launches = (int64_t)L.mt_first.size();
-  for (int g = 0; g < n_groups; ++g) g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
+  for (int g = 0; g < n_groups; ++g) {
+    g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
+    for (const Segment& sg : segs[g])
+      if (sg.pc_count) g_last_launches += 3LL * ticks[g];
+  }
 
   for (int g = 0; g < n_groups; ++g) {
     if (!use_graph) {
-      const int rc = launch_ticks(segs[g], dslots, ditems, ticks[g], tw, st);
+      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, ticks[g], tw, st);
       if (rc != SP_OK) return rc;
       continue;
     }
     GraphKey key{workspace_dev, dev, g, ticks[g], {}};
     for (const Segment& sg : segs[g])
-      key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1]});
+      key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1],
+                                         sg.pc_first, sg.pc_count, sg.pc_grid});
     cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);
@@ -398,7 +502,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     if (!exec) {
       cudaGraph_t graph = nullptr;
       SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const int rc = launch_ticks(segs[g], dslots, ditems, ticks[g], tw, st);
+      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, ticks[g], tw, st);
       const cudaError_t ce = cudaStreamEndCapture(st, &graph);
       if (rc != SP_OK) {
         if (graph) cudaGraphDestroy(graph);

@@ -44,6 +44,9 @@ struct Slot {
   const float* support;
   float2* save;
   double* err;
+  const float2* ipsf;      // partial coherence: transform of the point spread, or null
+  float2* w;               // divisor work plane of G's projection (partial coherence)
+  float2* w2;              // ... of G2's (DM)
 };
 
 struct Item {
@@ -532,13 +535,16 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
 
 // Is the slot live in the column pass at this tick (a projection, or the
 // random-phase start), and does it project (and so want its G tile)?
+// (Projections of partially coherent slots run in the sp_coherence kernels
+// instead; the column pass only builds their random-phase start.)
 __device__ __forceinline__ bool col_live(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
-  return step >= 0 && step <= s.n_iter && (step > 0 || s.init == SP_INIT_RANDOM_PHASE);
+  return step >= 0 && step <= s.n_iter &&
+         (step > 0 ? s.ipsf == nullptr : s.init == SP_INIT_RANDOM_PHASE);
 }
 __device__ __forceinline__ bool col_projects(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
-  return step >= 1 && step <= s.n_iter;
+  return step >= 1 && step <= s.n_iter && s.ipsf == nullptr;
 }
 
 // This thread's last-stage butterflies of a column item: butterfly u is row

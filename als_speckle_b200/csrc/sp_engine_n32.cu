@@ -1,8 +1,10 @@
-// Engine kernels and standalone 2-D FFT for N = 32 (see sp_engine_launch.cuh
-// and sp_fft2.cuh).
+// Engine kernels, standalone 2-D FFT and partial-coherence kernels for N = 32 (see
+// sp_engine_launch.cuh, sp_fft2.cuh and sp_coherence.cuh).
 #include "sp_engine_launch.cuh"
 #include "sp_fft2.cuh"
+#include "sp_coherence.cuh"
 namespace sp {
 SP_DEFINE_SIZE(32)
 SP_DEFINE_FFT2(32)
+SP_DEFINE_PC(32)
 }  // namespace sp

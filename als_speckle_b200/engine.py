@@ -73,6 +73,7 @@ class TrialSpec:
     save: Optional[torch.Tensor] = None    # complex64 (rows, cols) destination
     errors: Optional[torch.Tensor] = None  # float64 (iterations, 2) per-iteration sums
     quirks: str = "gpu"
+    ipsf: Optional[torch.Tensor] = None    # complex64 (N, N): partially coherent projection
 
     @property
     def n(self):
@@ -110,6 +111,11 @@ def _to_struct(t: TrialSpec) -> _lib.sp_trial:
         if t.errors.dtype != torch.float64 or t.errors.numel() < 2 * max(1, t.iterations) or not t.errors.is_contiguous():
             raise ValueError("errors must be a contiguous float64 tensor with 2*iterations entries")
         s.errors_dev = t.errors.data_ptr()
+    if t.ipsf is not None:
+        x = t.ipsf
+        if x.dtype != torch.complex64 or tuple(x.shape) != (N, N) or not x.is_cuda or not x.is_contiguous():
+            raise ValueError("ipsf must be a contiguous CUDA complex64 tensor of shape (%d, %d)" % (N, N))
+        s.ipsf_dev = x.data_ptr()
     return s
 
 

@@ -12,8 +12,10 @@ Differences from the reference, all deliberate:
   reference's CPU-branch forms instead (``phasing.py:1257``, ``:1284``).
 * Where ``|FFT(psi)| == 0`` the reference divides by zero
   (``phasing_fourier.cl:14``); here the modulus is kept with zero phase.
-* Partial-coherence inputs (``ipsf``, ``spectrum``) and ``debug_on`` FITS
-  dumps are not supported and raise.
+* The energy ``spectrum`` (longitudinal coherence, ``radial_rescale``) and
+  ``debug_on`` FITS dumps are not supported and raise.  ``ipsf`` (transverse
+  coherence) is supported; where its blurred divisor is 0 the modulus is kept
+  with zero phase, like the coherent case.
 """
 from __future__ import annotations
 
@@ -50,6 +52,7 @@ class phasing(common):
         self.modulus_state = 0
         self.support_state = 0
         self.ipsf_state = 0
+        self.ipsf = None
         self.buffer_state = 0
         self.spectrum_state = 0
         self.can_iterate = False
@@ -68,8 +71,8 @@ class phasing(common):
         for name, x in (("modulus", modulus), ("support", support), ("ipsf", ipsf)):
             if x is not None and not isinstance(x, np.ndarray):
                 raise TypeError("%s must be ndarray if supplied" % name)
-        if ipsf is not None or spectrum is not None:
-            raise NotImplementedError("partial-coherence projections (ipsf, spectrum) are not supported")
+        if spectrum is not None:
+            raise NotImplementedError("energy-spectrum (longitudinal coherence) projections are not supported")
         if modulus is not None:
             if modulus.ndim != 2:
                 raise ValueError("modulus must be 2d")
@@ -107,6 +110,20 @@ class phasing(common):
             self.numtrials = int(numtrials)
             if self.buffer_state == 0:
                 self.buffer_state = 1
+        # ipsf: transform of the coherence point spread, same shape as the
+        # modulus (phasing.py:413-424, dependency check :455-459)
+        if ipsf is not None:
+            if ipsf.ndim != 2 or ipsf.shape[0] != ipsf.shape[1]:
+                raise ValueError("ipsf must be a square 2d array")
+            ipsf = ipsf.astype(np.complex64)
+            if self.ipsf_state == 2 and ipsf.shape != tuple(self.ipsf.shape):
+                raise ValueError("ipsf shape %s differs from %s" % (ipsf.shape, tuple(self.ipsf.shape)))
+            self.ipsf = self._set(ipsf, self._allocate(ipsf.shape, np.complex64, "ipsf"))
+            self.ipsf_state = 1
+        if self.modulus_state == 2 and self.ipsf_state > 0:
+            if tuple(self.ipsf.shape) != self.shape:
+                raise ValueError("ipsf shape %s differs from the modulus %s" % (tuple(self.ipsf.shape), self.shape))
+            self.ipsf_state = 2
         if self.modulus_state == 2 and self.support_state > 0:
             sup = self._support_host
             if sup.shape != self.shape:
@@ -129,6 +146,10 @@ class phasing(common):
                     self.savebuffer = self._allocate(shape, np.complex64, "savebuffer")
                     self.buffer_state = 2
         self.can_iterate = self.modulus_state == 2 and self.support_state == 2 and self.buffer_state == 2
+
+    def _ipsf(self):
+        """The loaded ipsf when the projection is partially coherent, else None."""
+        return self.ipsf if self.ipsf_state == 2 else None
 
     # ------------------------------------------------------------------ seed
     def seed(self, val=None, supplied=None):
@@ -191,7 +212,7 @@ class phasing(common):
                              iterations=n, order=_runs_from_flat(rot), beta=beta,
                              box=(self.r0, self.c0, self.rows, self.cols) if last else None,
                              save=self.savebuffer[self.numtrial] if last else None,
-                             errors=self.errors[done:done + n], quirks="gpu")
+                             errors=self.errors[done:done + n], quirks="gpu", ipsf=self._ipsf())
             self.engine.solve([spec])
             done += n
             if silent is not True and (isinstance(silent, bool) or done % chunk == 0):
@@ -226,7 +247,8 @@ class phasing(common):
                                    random_phase=random_phase, seed=seed, trial=self.numtrial + k,
                                    box=(self.r0, self.c0, self.rows, self.cols),
                                    save=self.savebuffer[self.numtrial + k],
-                                   errors=errs[k] if errors else None, quirks=self.quirks))
+                                   errors=errs[k] if errors else None, quirks=self.quirks,
+                                   ipsf=self._ipsf()))
         self.engine.solve(specs)
         self.numtrial += trials
         return (psis, errs) if errors else psis

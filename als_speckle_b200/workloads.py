@@ -1,6 +1,6 @@
 """The benchmark workloads other than the headline batched HIO job.
 
-    python -m als_speckle_b200.workloads single256 | raar_dm1024 | uneven | serving [--out f.json]
+    python -m als_speckle_b200.workloads single256 | raar_dm1024 | uneven | serving | coherence512 [--out f.json]
 
 * ``single256``   one 256^2 trial, 200 HIO (beta 0.9) + 20 ER, random-phase start,
                    through ``phasing.iterate_trials``; final R-factor.
@@ -12,6 +12,9 @@
                    engine call versus one call per trial.
 * ``serving``     Poisson request stream through the continuous-batching
                    service; p50 / p99 latency, throughput, sustainable rate.
+* ``coherence512`` 32 x 512^2 trials, 200 HIO (beta 0.9), random-phase starts,
+                   with a partially coherent projection (Gaussian point spread,
+                   sigma 2 px) and without; trial-iterations/s of both.
 
 All inputs are seeded synthetic patterns (``synth``); results are printed as
 one JSON object.
@@ -171,9 +174,43 @@ def serving(rate=200.0, window=0.5, seed=0, budget_gb=120, chunk=64, sizes=(256,
             "sustainable_rate_per_s": capacity / work_per_req}
 
 
+def gaussian_ipsf(N, sigma):
+    """Transform of a normalised Gaussian point spread of ``sigma`` pixels,
+    corner-centred: the ``ipsf`` of ``phasing.load``."""
+    q = np.fft.fftfreq(N) * N
+    g = np.exp(-0.5 * (q[:, None] ** 2 + q[None, :] ** 2) / sigma ** 2)
+    return np.fft.fft2(g / g.sum()).astype(np.complex64)
+
+
+def coherence512(trials=32, iters=200, seed=0):
+    """Partially coherent against coherent projections on the same job."""
+    _, M, S = synth.config_pattern("hio_512x128", seed=seed)
+    N = M.shape[0]
+    dev = torch.device("cuda")
+    Md, Sd = torch.from_numpy(M).to(dev), torch.from_numpy(S).to(dev)
+    ipsf = torch.from_numpy(gaussian_ipsf(N, 2.0)).to(dev)
+    psis = torch.zeros((trials, N, N), dtype=torch.complex64, device=dev)
+    from . import autotune
+    eng = Engine(device=dev, use_graph=True, e_per_n={N: autotune.load_or_default(N)["E"]})
+    stream = torch.cuda.Stream()
+    out = {"workload": "coherence512", "trials": trials, "iterations": iters}
+    for name, ip in (("coherent", None), ("partially_coherent", ipsf)):
+        specs = [TrialSpec(psi=psis[k], modulus=Md, support=Sd, iterations=iters,
+                           order=(("hio", iters),), beta=0.9, random_phase=True, seed=seed,
+                           trial=k, ipsf=ip) for k in range(trials)]
+        with torch.cuda.stream(stream):
+            eng.solve(specs, stream=stream)  # warm-up (graph capture)
+            stream.synchronize()
+            _, dt = _timed(lambda: eng.solve(specs, stream=stream))
+        out[name + "_trial_iter_per_s"] = trials * iters / dt
+    eng.close()
+    out["ratio"] = out["partially_coherent_trial_iter_per_s"] / out["coherent_trial_iter_per_s"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=("single256", "raar_dm1024", "uneven", "serving"))
+    ap.add_argument("workload", choices=("single256", "raar_dm1024", "uneven", "serving", "coherence512"))
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--window", type=float, default=0.5)
     ap.add_argument("--rounds", type=int, default=None)
@@ -186,6 +223,8 @@ def main():
         r = raar_dm1024(rounds=a.rounds)
     elif a.workload == "uneven":
         r = uneven(iters=a.iters)
+    elif a.workload == "coherence512":
+        r = coherence512()
     else:
         r = serving(rate=a.rate, window=a.window)
     line = json.dumps(r)

@@ -76,6 +76,10 @@ typedef struct sp_trial {
   void* save_dev;                  /* complex64 rows*cols, receives the crop, or NULL */
   double* errors_dev;              /* 2*n_iter doubles (sum(|F|-M)^2, sum||F|-M|) per
                                       iteration, or NULL; zeroed by the run */
+  const void* ipsf_dev;            /* complex64 N*N transform of the coherence point spread,
+                                      corner-centred (phasing.load ipsf=, phasing.py:413-424;
+                                      divisor phasing.py:1122-1137), or NULL for a coherent
+                                      projection */
 } sp_trial;
 
 typedef struct sp_run_opts {
