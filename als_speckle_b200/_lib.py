@@ -94,6 +94,16 @@ _SIGS = {
     "sp_com_sums": ([_p, _i, _i, _i, _p, _p], _i),
     "sp_roll_accumulate": ([_p, _i, _i, _i, _p, _p, _p], _i),
     "sp_plain_iterate": ([_i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _p], _i),
+    "sp_abs2_f2_f2": ([_p, _p, _i64, _p], _i),
+    "sp_sqrt_f2": ([_p, _p, _i64, _p], _i),
+    "sp_sqrt_abs_f2": ([_p, _p, _i64, _p], _i),
+    "sp_multiply_axis_f_f2": ([_i, _p, _p, _p, _i64, _p], _i),
+    "sp_multiply_f2_f2": ([_p, _p, _p, _i64, _p], _i),
+    "sp_rftf_accumulate": ([_i, _p, _p, _p, _i, _i, _p], _i),
+    "sp_rftf_map": ([_p, _p, _i, _i, _p, _p, _p, _p], _i),
+    "sp_rftf_from_error": ([_p, _p, _i64, _i, _p], _i),
+    "sp_remove_hot_pixels": ([_p, _p, _i, _i, _i, _i, _f, _p], _i),
+    "sp_covar_pairs": ([_p, _i, _p, _i, _p, _i, _p, _p], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(lib, _name)

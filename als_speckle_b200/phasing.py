@@ -19,6 +19,7 @@ Differences from the reference, all deliberate:
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -471,9 +472,164 @@ def fft2(x, inverse=False):
     return out
 
 
-def rftf(*args, **kwargs):
-    raise NotImplementedError("rftf is not part of this engine yet")
+def _pow2_size(N, who):
+    if N & (N - 1) or not 8 <= N <= 4096:
+        raise ValueError("%s: N=%d must be a power of two in [8, 4096]" % (who, N))
 
 
-def covar_results(*args, **kwargs):
-    raise NotImplementedError("covar_results is not part of this engine yet")
+def _embed(frames, N):
+    """Frames (F, r, c) placed at the corner of zeroed (F, N, N) planes."""
+    F, r, c = frames.shape
+    if r > N or c > N:
+        raise ValueError("estimate must be smaller than goal_modulus")
+    out = torch.zeros((F, N, N), dtype=torch.complex64, device=frames.device)
+    out[:, :r, :c] = frames
+    return out
+
+
+def _hot_pixels(x, threshold, iterations=1):
+    """remove_hot_pixels on a device float32 array (2d or 3d), in place."""
+    rows, cols = x.shape[-2], x.shape[-1]
+    frames = x.numel() // (rows * cols)
+    work = torch.empty((rows, cols), dtype=torch.float32, device=x.device)
+    call("sp_remove_hot_pixels", ptr(x), ptr(work), frames, rows, cols, iterations,
+         C.c_float(threshold), stream_ptr())
+    return x
+
+
+def remove_hot_pixels(data_in, iterations=1, threshold=2, gpu_info=None):
+    """``conditioning.remove_hot_pixels`` (``conditioning.py:207-313``): pixels
+    above ``threshold`` times the local 3 x 3 median (+0.1) are replaced by
+    it, ``iterations`` times; ``gpu_info`` is ignored."""
+    was_np = isinstance(data_in, np.ndarray)
+    x = torch.from_numpy(np.ascontiguousarray(data_in, np.float32)).cuda() if was_np else \
+        data_in.to(torch.float32).contiguous().clone()
+    if x.dim() not in (2, 3):
+        raise ValueError("data must be 2d or 3d")
+    _hot_pixels(x, threshold, iterations)
+    return x.cpu().numpy() if was_np else x
+
+
+def rftf(estimate, goal_modulus, hot_pixels=False, ipsf=None, rftfq=False, scale=False):
+    """RFTF of one estimate against the goal modulus (``phasing.py:1521-1608``):
+    the speckle modulus of the estimate embedded at the corner (blurred by
+    ``ipsf`` if given: the modulus is convolved, as the reference's numpy
+    function does), lined up with the goal (centred at (0,0) or (N/2,N/2),
+    whichever fits better), ``sqrt(1/(1+(F-g)^2/g^2))`` in the centred layout,
+    optionally rescaled to [0, 1] and cleaned of hot pixels.  N must be a
+    power of two here.  ``rftfq`` adds the annular mean about the centre."""
+    est, was_np, _ = _device_frames(estimate)
+    g = torch.from_numpy(np.ascontiguousarray(goal_modulus, np.float32)).cuda() \
+        if isinstance(goal_modulus, np.ndarray) else goal_modulus.to(torch.float32).contiguous()
+    N = int(g.shape[0])
+    _pow2_size(N, "rftf")
+    if g.shape != (N, N):
+        raise ValueError("goal_modulus must be square")
+    st = stream_ptr()
+    f = _embed(est[:1], N)
+    call("sp_fft2", ptr(f), ptr(f), N, 1, 0, st)
+    call("sp_abs_f2_f2", ptr(f), ptr(f), N * N, st)
+    if ipsf is not None:
+        ip = torch.from_numpy(np.ascontiguousarray(ipsf, np.complex64)).cuda() \
+            if isinstance(ipsf, np.ndarray) else ipsf.to(torch.complex64).contiguous()
+        if tuple(ip.shape) != (N, N):
+            raise ValueError("ipsf must have the goal modulus' shape")
+        call("sp_fft2", ptr(f), ptr(f), N, 1, 0, st)
+        call("sp_multiply_f2_f2", ptr(f), ptr(ip), ptr(f), N * N, st)
+        call("sp_fft2", ptr(f), ptr(f), N, 1, 1, st)
+        call("sp_sqrt_abs_f2", ptr(f), ptr(f), N * N, st)
+    sums = torch.empty(2, dtype=torch.float64, device=g.device)
+    err = torch.empty((N, N), dtype=torch.float32, device=g.device)
+    out = torch.empty((N, N), dtype=torch.float32, device=g.device)
+    call("sp_rftf_map", ptr(f), ptr(g), N, 1 if scale else 0, ptr(sums), ptr(err), ptr(out), st)
+    if hot_pixels:
+        _hot_pixels(err, 2.0)
+        call("sp_rftf_from_error", ptr(err), ptr(out), N * N, 1 if scale else 0, st)
+        _hot_pixels(out, 1.1)
+    res = out.cpu().numpy() if was_np else out
+    if rftfq:
+        return res, _annular_average(out.cpu().numpy())
+    return res
+
+
+def gpu_rftf(gpuinfo, estimates, goal_modulus, ipsf=None, rftfq=False):
+    """``phasing.gpu_rftf`` (``phasing.py:1611-1708``) over many estimates:
+    each estimate's transform F (with ``ipsf``: the intensity |F|^2 blurred
+    by the real part of ipsf, then the principal square root), then the mean
+    over estimates of ``1/sqrt(1 + (g - Re F)^2/g^2)``, fftshifted.
+    ``gpuinfo`` is ignored."""
+    est, was_np, _ = _device_frames(estimates)
+    g = torch.from_numpy(np.ascontiguousarray(goal_modulus, np.float32)).cuda() \
+        if isinstance(goal_modulus, np.ndarray) else goal_modulus.to(torch.float32).contiguous()
+    N = int(g.shape[0])
+    _pow2_size(N, "gpu_rftf")
+    L = est.shape[0]
+    st = stream_ptr()
+    f = _embed(est, N)
+    call("sp_fft2", ptr(f), ptr(f), N, L, 0, st)
+    if ipsf is not None:
+        ip = np.real(np.asarray(ipsf)).astype(np.float32) if not isinstance(ipsf, torch.Tensor) \
+            else ipsf.real.cpu().numpy().astype(np.float32)
+        ipd = torch.from_numpy(np.ascontiguousarray(ip)).cuda()
+        call("sp_abs2_f2_f2", ptr(f), ptr(f), f.numel(), st)
+        call("sp_fft2", ptr(f), ptr(f), N, L, 0, st)
+        call("sp_multiply_axis_f_f2", L, ptr(ipd), ptr(f), ptr(f), N * N, st)
+        call("sp_fft2", ptr(f), ptr(f), N, L, 1, st)
+        call("sp_sqrt_f2", ptr(f), ptr(f), f.numel(), st)
+    else:
+        call("sp_abs_f2_f2", ptr(f), ptr(f), f.numel(), st)
+    acc = torch.empty((N, N), dtype=torch.float32, device=g.device)
+    call("sp_rftf_accumulate", L, ptr(g), ptr(acc), ptr(f), N, 1, st)
+    res = acc.cpu().numpy() if was_np else acc
+    if rftfq:
+        return res, _annular_average(acc.cpu().numpy())
+    return res
+
+
+def covar_results(gpuinfo, data, threshold=0.85, mask=None):
+    """Pair-wise similarity of reconstructions for configuration sorting
+    (``phasing.py:1817-1982``): frames zero-padded to N x N (the larger edge
+    if a power of two, else 2**(round(log2 edge) + 1), as ``_reshape_data``
+    computes it), their transforms D, cc[n, m] = max |IFFT2(conj(D_n) D_m)|
+    for the pairs the mask selects, covars = cc/sqrt(cc_nn cc_mm) (NaN -> 0),
+    and per-row stats (row, mean covariance, count above ``threshold``).
+    ``mask``: an array, or a float p drawing a random pair mask with numpy's
+    global RNG as the reference does (default 1.0: every pair).  Returns
+    (cc, covars, stats, transforms).  The reference's own version cannot run
+    (it reads an undefined ``self``); ``gpuinfo`` is ignored."""
+    data = np.asarray(data)
+    if data.ndim != 3:
+        raise ValueError("data must be 3d")
+    frames, rows, cols = data.shape
+    e = max(rows, cols)
+    N = e if e & (e - 1) == 0 else 2 ** (int(round(np.log2(e))) + 1)
+    _pow2_size(N, "covar_results")
+    if mask is None:
+        mask = 1.0
+    if not isinstance(mask, np.ndarray):
+        mask = np.where(np.random.rand(frames, frames) < mask, 1, 0)
+    d = torch.zeros((frames, N, N), dtype=torch.complex64, device="cuda")
+    d[:, :rows, :cols] = torch.from_numpy(np.ascontiguousarray(data.astype(np.complex64))).cuda()
+    st = stream_ptr()
+    call("sp_fft2", ptr(d), ptr(d), N, frames, 0, st)
+    pairs = [(n, m) for n in range(frames) for m in (np.nonzero(mask[n, n:])[0] + n)]
+    cc = np.zeros((frames, frames))
+    if pairs:
+        pr = torch.tensor(pairs, dtype=torch.int32, device="cuda").contiguous()
+        planes = max(1, min(len(pairs), (512 << 20) // (N * N * 8)))
+        work = torch.empty((planes, N, N), dtype=torch.complex64, device="cuda")
+        vals = torch.empty(len(pairs), dtype=torch.float32, device="cuda")
+        call("sp_covar_pairs", ptr(d), N, ptr(pr), len(pairs), ptr(work), planes, ptr(vals), st)
+        for (n, m), v in zip(pairs, vals.cpu().numpy().astype(np.float64)):
+            cc[n, m] = cc[m, n] = v
+    covars = np.zeros((frames, frames))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for n, m in pairs:
+            covars[n, m] = covars[m, n] = cc[n, m] / np.sqrt(cc[n, n] * cc[m, m])
+    covars = np.nan_to_num(covars)
+    stats = None
+    if threshold > 0:
+        stats = np.zeros((frames, 3))
+        for row in range(frames):
+            stats[row] = row, np.average(covars[row]), np.sum(covars[row] > threshold)
+    return cc, covars, stats, d.cpu().numpy()

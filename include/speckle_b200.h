@@ -209,6 +209,42 @@ int sp_com_sums(const void* frames_dev, int n_frames, int rows, int cols, double
 int sp_roll_accumulate(const void* frames_dev, int n_frames, int rows, int cols,
                        const int* shifts_dev, void* out_dev, sp_stream_t stream);
 
+/* ---- trial quality: RFTF, hot pixels, pair-wise covariances ------------- */
+/* (|x|^2, 0)  -- kernels/common_abs2_f2_f2.cl */
+int sp_abs2_f2_f2(const void* in_dev, void* out_dev, int64_t n, sp_stream_t stream);
+/* principal complex square root  -- kernels/common_sqrt_f2.cl */
+int sp_sqrt_f2(const void* in_dev, void* out_dev, int64_t n, sp_stream_t stream);
+/* (sqrt(|x|), 0): the CPU rftf's blurred modulus (phasing.py:1577) */
+int sp_sqrt_abs_f2(const void* in_dev, void* out_dev, int64_t n, sp_stream_t stream);
+/* out[f] = in1 * in2[f], in1 real  -- kernels/common_multiply_axis_f_f2.cl */
+int sp_multiply_axis_f_f2(int frames, const float* in1_dev, const void* in2_dev, void* out_dev,
+                          int64_t plane, sp_stream_t stream);
+/* out = a * b, complex  -- kernels/common_multiply_f2_f2.cl */
+int sp_multiply_f2_f2(const void* a_dev, const void* b_dev, void* out_dev, int64_t n,
+                      sp_stream_t stream);
+/* gpu_rftf's accumulation (phasing.py:1611-1708, kernels/phasing_rftf_accumulate.cl):
+ * acc = mean over frames of 1/sqrt(1 + (g - Re F)^2/g^2), written fftshifted if shift. */
+int sp_rftf_accumulate(int frames, const float* goal_dev, float* accumulation_dev,
+                       const void* fourier_dev, int N, int shift, sp_stream_t stream);
+/* rftf's error map for one estimate (phasing.py:1583-1601): picks the goal's centring from
+ * the FP64 sums |F - g| and |shift(F) - g| (sums_dev: 2 doubles, read back), writes the
+ * centred error err_dev and out_dev = sqrt(1/(1+err)) (rescaled to [0,1] if scale). */
+int sp_rftf_map(const void* fourier_dev, const float* goal_dev, int N, int scale, double* sums_dev,
+                float* err_dev, float* out_dev, sp_stream_t stream);
+/* out = sqrt(1/(1+err)), rescaled if scale (phasing.py:1597-1601) */
+int sp_rftf_from_error(const float* err_dev, float* out_dev, int64_t n, int scale,
+                       sp_stream_t stream);
+/* conditioning.remove_hot_pixels, CPU branch (conditioning.py:304-305): per frame and
+ * iteration, median = medfilt 3x3 (zero padding) + 0.1; data = median where
+ * data/median > threshold.  work_dev: rows*cols floats. */
+int sp_remove_hot_pixels(float* data_dev, float* work_dev, int frames, int rows, int cols,
+                         int iterations, float threshold, sp_stream_t stream);
+/* covar_results (phasing.py:1817-1982): cc[p] = max |IFFT2(conj(D_a) D_b)| for each pair
+ * p = (a, b) of pairs_dev (int32 pairs) of transformed frames dfts_dev (N*N complex64 each);
+ * work_dev holds work_planes N*N complex64 planes, pairs are done that many at a time. */
+int sp_covar_pairs(const void* dfts_dev, int N, const int32_t* pairs_dev, int n_pairs,
+                   void* work_dev, int work_planes, float* cc_dev, sp_stream_t stream);
+
 /* ---- plain single-instance path (the reference's GPU dataflow) --------- */
 /* One trial, cuFFT C2C plans plus one elementwise kernel per step with a
  * stream synchronisation after each, as phasing.py:1187-1353 drives pyfft and

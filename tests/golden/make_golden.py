@@ -195,12 +195,40 @@ def coherence():
     np.savez_compressed(os.path.join(HERE, "coherence.npz"), **out)
 
 
+def quality():
+    """rftf (phasing.py:1521-1608) and remove_hot_pixels
+    (conditioning.py:207-313) of the reference's numpy path."""
+    out = {}
+    for N in (32, 64):
+        rng = np.random.default_rng(500 + N)
+        B = N // 4
+        obj = np.zeros((N, N), np.complex128)
+        obj[:B, :B] = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.5, 0.5, (B, B)))
+        goal = (np.abs(np.fft.fft2(obj)) + 0.05).astype(np.float32)
+        est = (obj[:B, :B] + 0.05 * rng.standard_normal((B, B))).astype(np.complex64)
+        ipsf = gaussian_ipsf(N, 1.5)
+        out["N%d_goal" % N], out["N%d_est" % N], out["N%d_ipsf" % N] = goal, est, ipsf
+        out["N%d_plain" % N] = ref.phasing.rftf(est, goal)
+        out["N%d_centred" % N] = ref.phasing.rftf(est, np.fft.fftshift(goal))
+        out["N%d_ipsf_out" % N] = ref.phasing.rftf(est, goal, ipsf=ipsf)
+        out["N%d_scale" % N] = ref.phasing.rftf(est, goal, scale=True)
+        out["N%d_hot" % N] = ref.phasing.rftf(est, goal, hot_pixels=True)
+        # (rftfq=True cannot run under Python 3: N/2 is a float in wrapping.unwrap)
+        frames = (rng.random((2, N, N)) * 3).astype(np.float32)
+        frames[0, 5, 7] = 40.0
+        frames[1, N - 1, 0] = 25.0
+        out["N%d_hp_in" % N] = frames
+        out["N%d_hp_out" % N] = ref.conditioning.remove_hot_pixels(frames.copy(), iterations=2)
+    np.savez_compressed(os.path.join(HERE, "quality.npz"), **out)
+
+
 if __name__ == "__main__":
     projections()
     trajectories()
     seeds()
     helpers()
     coherence()
+    quality()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
