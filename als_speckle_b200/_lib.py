@@ -43,6 +43,8 @@ class sp_trial(C.Structure):
         ("r0", C.c_int32), ("c0", C.c_int32), ("rows", C.c_int32), ("cols", C.c_int32),
         ("psi_dev", C.c_void_p), ("modulus_dev", C.c_void_p), ("support_dev", C.c_void_p),
         ("save_dev", C.c_void_p), ("errors_dev", C.c_void_p), ("ipsf_dev", C.c_void_p),
+        ("spectrum_rescale_dev", C.c_void_p), ("spectrum_weight_dev", C.c_void_p),
+        ("spectrum_n", C.c_int32),
     ]
 
 

@@ -1,13 +1,21 @@
-// Partially coherent projection (load(ipsf=...), phasing.py:1109-1137 and
-// :1187-1228): the modulus is replaced with the divisor
-//     div = sqrt(|IFFT2(FFT2(|F|^2) * ipsf)|),    F = FFT2(psi),
-// i.e. |F| blurred by the coherence function whose transform is ipsf.  The
-// divisor needs the whole 2-D |F|^2, so for these slots the engine's column
-// pass is replaced by three launches per projection plane (G, and G2 for DM):
-//   A (columns)  F = FFT_cols(G), stored over G;  W = FFT_cols(|F|^2)
-//   W (rows)     W = IFFT_rows(FFT_rows(W) * ipsf)           (unnormalised)
-//   B (columns)  div = sqrt(|IFFT_cols(W)|) / N;  P = M F / div;
-//                G = conj(IFFT_cols(P / N^2)) = FFT_cols(conj(P) / N^2)
+// Partially coherent projections: the modulus replacement of
+// phasing.py:1187-1228 with the divisor built by _build_divisor
+// (phasing.py:1109-1157, GPU branch):
+//   ipsf (transverse coherence, load(ipsf=...)):
+//       div = sqrt(|IFFT2(FFT2(|F|^2) * ipsf)|),    F = FFT2(psi)
+//   spectrum (longitudinal coherence, load(spectrum=...)), after the above:
+//       div = sqrt(radial_rescale(div^2))   (kernels/phasing_radial_rescale.cl)
+// The divisor needs the whole 2-D |F|^2, so for these slots the engine's
+// column pass is replaced by up to five launches per projection plane (G,
+// and G2 for DM), each skipping the jobs it does not apply to:
+//   A  (columns) F = FFT_cols(G), stored over G; then W = FFT_cols(|F|^2)
+//                (ipsf) or P = |F|^2 (spectrum only)
+//   W  (rows)    W = IFFT_rows(FFT_rows(W) * ipsf), unnormalised   [ipsf]
+//   B1 (columns) P = |IFFT_cols(W)| / N^2                     [ipsf + spectrum]
+//   R            W (as floats) = radial_rescale(P)                [spectrum]
+//   B  (columns) div = sqrt(|IFFT_cols(W)|) / N (ipsf only) or sqrt(W floats)
+//                (spectrum); P = M F / div; G = conj(IFFT_cols(P / N^2))
+//                = FFT_cols(conj(P) / N^2)
 // B leaves G conjugated, as the engine's row pass expects.  The lines are
 // transformed with the engine's Stockham building blocks, E = min(16, N)
 // values per thread, one item (C columns or L rows of one plane) per block
@@ -71,6 +79,14 @@ __global__ void __launch_bounds__(kThreads) pc_cols_a_kernel(PcArgs a) {
         v[i] = make_float2(v[i].x * v[i].x + v[i].y * v[i].y, 0.f);
       }
     }
+    if (s.ipsf == nullptr) {  // spectrum only: the squared divisor is |F|^2
+      float* pp = job.y ? s.p2 : s.p;
+      if (active) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) pp[off + (size_t)i * T * N] = v[i].x;
+      }
+      continue;
+    }
     fft_line<N, E, -1>(v, lay, BlockSync{}, active, t, tw);
     if (active) {
 #pragma unroll
@@ -97,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) pc_rows_w_kernel(PcArgs a) {
     const int j = it / PER, blk = it - j * PER;
     const int2 job = a.jobs[j];
     const Slot& s = a.slots[job.x];
-    if (!pc_active(s, job.y, a.tick)) continue;
+    if (!pc_active(s, job.y, a.tick) || s.ipsf == nullptr) continue;
     float2* w = job.y ? s.w2 : s.w;
     const size_t off = (size_t)(blk * L + lr) * N + t;
     float2 v[E];
@@ -145,15 +161,24 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
     float2 v[E];
     float dv[E];
     __syncthreads();
-    if (active) {
+    const bool spec = s.spec_n > 0;
+    if (!spec) {
+      if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) v[i] = w[off + (size_t)i * T * N];
+        for (int i = 0; i < E; ++i) v[i] = w[off + (size_t)i * T * N];
+      }
+      fft_line<N, E, +1>(v, lay, BlockSync{}, active, t, tw);
     }
-    fft_line<N, E, +1>(v, lay, BlockSync{}, active, t, tw);
     float f2 = 0.f, f1 = 0.f;
     if (active) {
+      if (spec) {  // R left the rescaled squared divisor in W, read as floats
+        const float* wf = reinterpret_cast<const float*>(w);
 #pragma unroll
-      for (int i = 0; i < E; ++i) dv[i] = sqrtf(sqrtf(v[i].x * v[i].x + v[i].y * v[i].y)) * inv_n;
+        for (int i = 0; i < E; ++i) dv[i] = sqrtf(wf[off + (size_t)i * T * N]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < E; ++i) dv[i] = sqrtf(sqrtf(v[i].x * v[i].x + v[i].y * v[i].y)) * inv_n;
+      }
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const float2 f = g[off + (size_t)i * T * N];
@@ -186,12 +211,95 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
   }
 }
 
-// which: 0 = A, 1 = W, 2 = B
+// B1: P = |IFFT_cols(W)| / N^2, the squared ipsf divisor, for slots that
+// also have a spectrum.
+template <int N>
+__global__ void __launch_bounds__(kThreads) pc_cols_b1_kernel(PcArgs a) {
+  constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
+  constexpr float inv = 1.0f / ((float)N * (float)N);
+  extern __shared__ float2 smem[];
+  float2* tw = smem + item_smem_elems(N, E);
+  build_stage_twiddles<N, E>(tw, a.tw + N);
+  const int tid = threadIdx.x, c = tid % C, t = tid / C;
+  const bool active = t < T;
+  const ColLayout<pad_shift(E), C> lay{smem + c};
+  constexpr int PER = N / C;
+  for (int it = blockIdx.x; it < a.n_jobs * PER; it += gridDim.x) {
+    const int j = it / PER, blk = it - j * PER;
+    const int2 job = a.jobs[j];
+    const Slot& s = a.slots[job.x];
+    if (!pc_active(s, job.y, a.tick) || s.ipsf == nullptr || s.spec_n == 0) continue;
+    const float2* w = job.y ? s.w2 : s.w;
+    float* pp = job.y ? s.p2 : s.p;
+    const size_t off = (size_t)(active ? t : 0) * N + blk * C + c;
+    float2 v[E];
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = w[off + (size_t)i * T * N];
+    }
+    fft_line<N, E, +1>(v, lay, BlockSync{}, active, t, tw);
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) pp[off + (size_t)i * T * N] = sqrtf(v[i].x * v[i].x + v[i].y * v[i].y) * inv;
+    }
+  }
+}
+
+// R: W (read as N*N floats) = radial_rescale(P)  -- phasing_radial_rescale.cl:
+// out(x, y) = sum_k w_k * bilinear(P, x / r_k, y / r_k) with corner-centred
+// coordinates (x = i or i - N for column i, y likewise for row j); taps at
+// or beyond -N/2 and N/2 carry weight 0 and are not read (the reference
+// reads them, possibly outside the array, and multiplies by 0).
+template <int N>
+__global__ void __launch_bounds__(kThreads) pc_rescale_kernel(PcArgs a) {
+  constexpr int N2 = N / 2;
+  constexpr int64_t PLANE = (int64_t)N * N;
+  for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < a.n_jobs * PLANE;
+       it += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(it / PLANE);
+    const int64_t k = it - (int64_t)j * PLANE;
+    const int2 job = a.jobs[j];
+    const Slot& s = a.slots[job.x];
+    if (!pc_active(s, job.y, a.tick) || s.spec_n == 0) continue;
+    const float* pp = job.y ? s.p2 : s.p;
+    float* out = reinterpret_cast<float*>(job.y ? s.w2 : s.w);
+    const int row = (int)(k / N), col = (int)(k - (int64_t)row * N);
+    const float x = (float)(col > N2 - 1 ? col - N : col);
+    const float y = (float)(row > N2 - 1 ? row - N : row);
+    float cum = 0.f;
+    for (int q = 0; q < s.spec_n; ++q) {
+      const float rv = s.spec_r[q], sw = s.spec_w[q];
+      const float rx = x / rv, ry = y / rv;
+      const int x1 = (int)floorf(rx), y1 = (int)floorf(ry);
+      const int x2 = x1 + 1, y2 = y1 + 1;
+      const bool kx1 = x1 > -N2 && x1 < N2, kx2 = x2 > -N2 && x2 < N2;
+      const bool ky1 = y1 > -N2 && y1 < N2, ky2 = y2 > -N2 && y2 < N2;
+      const float wx1 = kx1 ? 1.f - fabsf((float)x1 - rx) : 0.f;
+      const float wx2 = kx2 ? 1.f - fabsf((float)x2 - rx) : 0.f;
+      const float wy1 = ky1 ? 1.f - fabsf((float)y1 - ry) : 0.f;
+      const float wy2 = ky2 ? 1.f - fabsf((float)y2 - ry) : 0.f;
+      const int c1 = x1 < 0 ? x1 + N : x1, c2 = x2 < 0 ? x2 + N : x2;
+      const int r1 = y1 < 0 ? y1 + N : y1, r2 = y2 < 0 ? y2 + N : y2;
+      const float v11 = (kx1 && ky1) ? pp[(int64_t)r1 * N + c1] : 0.f;
+      const float v12 = (kx1 && ky2) ? pp[(int64_t)r2 * N + c1] : 0.f;
+      const float v21 = (kx2 && ky1) ? pp[(int64_t)r1 * N + c2] : 0.f;
+      const float v22 = (kx2 && ky2) ? pp[(int64_t)r2 * N + c2] : 0.f;
+      const float iv = v11 * wx1 * wy1 + v12 * wx1 * wy2 + v21 * wx2 * wy1 + v22 * wx2 * wy2;
+      cum += iv * sw;
+    }
+    out[k] = cum;
+  }
+}
+
+// which: 0 = A, 1 = W, 2 = B1, 3 = R, 4 = B
 template <int N>
 cudaError_t launch_pc_t(int which, int grid, cudaStream_t st, const PcArgs& a) {
   const size_t sm = (size_t)pc_smem_elems<N>() * sizeof(float2);
   if (which == 0) pc_cols_a_kernel<N><<<grid, kThreads, sm, st>>>(a);
   else if (which == 1) pc_rows_w_kernel<N><<<grid, kThreads, sm, st>>>(a);
+  else if (which == 2) pc_cols_b1_kernel<N><<<grid, kThreads, sm, st>>>(a);
+  else if (which == 3) pc_rescale_kernel<N><<<grid, kThreads, 0, st>>>(a);
   else pc_cols_b_kernel<N><<<grid, kThreads, sm, st>>>(a);
   return cudaGetLastError();
 }
@@ -202,6 +310,8 @@ cudaError_t pc_setup_t() {
   cudaError_t e = cudaFuncSetAttribute(pc_cols_a_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(pc_rows_w_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(pc_cols_b1_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(pc_cols_b_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }

@@ -141,6 +141,9 @@ static bool uses_dm(const sp_trial& t) {
   return false;
 }
 
+// Does the trial project with a partially coherent divisor (ipsf and/or spectrum)?
+static bool partial(const sp_trial& t) { return t.ipsf_dev != nullptr || t.spectrum_n > 0; }
+
 static int default_e(int N) { return N >= 32 ? 32 : N; }
 
 static int chosen_e(int N, const sp_run_opts* opts) {
@@ -173,6 +176,10 @@ static int validate(const sp_trial& t, int idx) {
            SP_ERR_INVALID, "trial %d: psi, modulus, support and ipsf must be 16-byte aligned", idx);
   SP_CHECK(t.init == SP_INIT_GIVEN || t.init == SP_INIT_RANDOM_PHASE, SP_ERR_INVALID,
            "trial %d: unknown init mode %d", idx, t.init);
+  SP_CHECK(t.spectrum_n >= 0 && t.spectrum_n <= 65536, SP_ERR_INVALID,
+           "trial %d: spectrum_n=%d", idx, t.spectrum_n);
+  SP_CHECK(t.spectrum_n == 0 || (t.spectrum_rescale_dev && t.spectrum_weight_dev), SP_ERR_INVALID,
+           "trial %d: spectrum pointers are required when spectrum_n > 0", idx);
   if (uses_dm(t)) SP_CHECK(t.beta != 0.f, SP_ERR_INVALID, "trial %d: DM needs beta != 0", idx);
   if (t.save_dev) {
     SP_CHECK(t.r0 >= 0 && t.c0 >= 0 && t.rows > 0 && t.cols > 0 && t.r0 + t.rows <= t.n &&
@@ -189,6 +196,7 @@ struct Layout {
   std::vector<size_t> mt_off;  // transposed modulus of each trial (shared by equal moduli)
   std::vector<int> mt_first;   // trials that own a transposed modulus (first use)
   std::vector<size_t> w_off, w2_off;  // partial-coherence divisor planes (0 = none)
+  std::vector<size_t> p_off, p2_off;  // squared-divisor planes of spectrum trials (0 = none)
   size_t jobs_off;             // (slot, plane) jobs of the partial-coherence kernels
   int n_items, n_jobs;
 };
@@ -208,7 +216,7 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
   L.n_items = items;
   int jobs = 0;
   for (int i = 0; i < n; ++i)
-    if (trials[i].ipsf_dev) jobs += uses_dm(trials[i]) ? 2 : 1;
+    if (partial(trials[i])) jobs += uses_dm(trials[i]) ? 2 : 1;
   L.n_jobs = jobs;
   L.jobs_off = L.items_off + align_up(sizeof(Item) * (size_t)std::max(items, 1));
   L.planes_off = L.jobs_off + align_up(sizeof(int2) * (size_t)std::max(jobs, 1));
@@ -228,14 +236,25 @@ static Layout layout_for(const sp_trial* trials, int n, const sp_run_opts* opts)
   // divisor planes of partially coherent trials, one per projection plane
   L.w_off.assign(n, 0);
   L.w2_off.assign(n, 0);
+  L.p_off.assign(n, 0);
+  L.p2_off.assign(n, 0);
   for (int i = 0; i < n; ++i) {
-    if (!trials[i].ipsf_dev) continue;
-    const size_t plane = (size_t)trials[i].n * trials[i].n * sizeof(float2);
+    if (!partial(trials[i])) continue;
+    const size_t px = (size_t)trials[i].n * trials[i].n;
+    const bool dm = uses_dm(trials[i]), spec = trials[i].spectrum_n > 0;
     L.w_off[i] = off;
-    off += align_up(plane);
-    if (uses_dm(trials[i])) {
+    off += align_up(px * sizeof(float2));
+    if (dm) {
       L.w2_off[i] = off;
-      off += align_up(plane);
+      off += align_up(px * sizeof(float2));
+    }
+    if (spec) {
+      L.p_off[i] = off;
+      off += align_up(px * sizeof(float));
+      if (dm) {
+        L.p2_off[i] = off;
+        off += align_up(px * sizeof(float));
+      }
     }
   }
   // one transposed copy per distinct (modulus, N), for the column pass
@@ -286,6 +305,7 @@ static cudaError_t launch_transpose(const float* src, float* dst, int N, cudaStr
 struct Segment {
   int N, E, first, count, grid[2];  // grid[pass]: 0 column, 1 row
   int pc_first, pc_count, pc_grid;  // partial-coherence jobs of this size
+  int pc_egrid;                     // grid of the elementwise rescale kernel
 };
 
 struct GraphKey {
@@ -308,7 +328,8 @@ static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, con
     for (const Segment& sg : segs) {
       if (sg.pc_count == 0) continue;
       PcArgs pa{slots, jobs + sg.pc_first, sg.pc_count, k, tw};
-      for (int which = 0; which < 3; ++which) SP_CUDA_TRY(launch_pc(sg.N, which, sg.pc_grid, st, pa));
+      for (int which = 0; which < 5; ++which)
+        SP_CUDA_TRY(launch_pc(sg.N, which, which == 3 ? sg.pc_egrid : sg.pc_grid, st, pa));
     }
     for (int which = 0; which < 2; ++which) {
       for (const Segment& sg : segs) {
@@ -394,14 +415,14 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       if (count == 0) continue;
       int occ[2] = {1, 1}, sms = 1;
       SP_CUDA_TRY(occupancy_for(N, E, occ, &sms));
-      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1};
+      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1, 1};
       for (int p = 0; p < 2; ++p) {
         int per_sm = occ[p];
         if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
         sg.grid[p] = std::max(1, std::min(count, sms * per_sm));
       }
       for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
-        if (trials[i].n != N || !trials[i].ipsf_dev) continue;
+        if (trials[i].n != N || !partial(trials[i])) continue;
         hj.push_back(int2{i, 0});
         if (uses_dm(trials[i])) hj.push_back(int2{i, 1});
       }
@@ -410,6 +431,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
         SP_CUDA_TRY(pc_ready(N));
         const int per_job = N / lines_per_item(N, pc_e(N));
         sg.pc_grid = std::max(1, std::min(sg.pc_count * per_job, sms * 4));
+        const int64_t ew = ((int64_t)sg.pc_count * N * N + 255) / 256;
+        sg.pc_egrid = (int)std::max<int64_t>(1, std::min<int64_t>(ew, (int64_t)sms * 16));
       }
       segs[g].push_back(sg);
     }
@@ -449,6 +472,11 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       s.ipsf = static_cast<const float2*>(t.ipsf_dev);
       s.w = L.w_off[i] ? reinterpret_cast<float2*>(ws + L.w_off[i]) : nullptr;
       s.w2 = L.w2_off[i] ? reinterpret_cast<float2*>(ws + L.w2_off[i]) : nullptr;
+      s.spec_n = t.spectrum_n;
+      s.spec_r = t.spectrum_n ? t.spectrum_rescale_dev : nullptr;
+      s.spec_w = t.spectrum_n ? t.spectrum_weight_dev : nullptr;
+      s.p = L.p_off[i] ? reinterpret_cast<float*>(ws + L.p_off[i]) : nullptr;
+      s.p2 = L.p2_off[i] ? reinterpret_cast<float*>(ws + L.p2_off[i]) : nullptr;
     }
   }
   SP_CHECK((int)hi.size() <= L.n_items, SP_ERR_INVALID,
@@ -480,7 +508,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
   for (int g = 0; g < n_groups; ++g) {
     g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
     for (const Segment& sg : segs[g])
-      if (sg.pc_count) g_last_launches += 3LL * ticks[g];
+      if (sg.pc_count) g_last_launches += 5LL * ticks[g];
   }
 
   for (int g = 0; g < n_groups; ++g) {
@@ -492,7 +520,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     GraphKey key{workspace_dev, dev, g, ticks[g], {}};
     for (const Segment& sg : segs[g])
       key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1],
-                                         sg.pc_first, sg.pc_count, sg.pc_grid});
+                                         sg.pc_first, sg.pc_count, sg.pc_grid, sg.pc_egrid});
     cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);

@@ -47,6 +47,12 @@ struct Slot {
   const float2* ipsf;      // partial coherence: transform of the point spread, or null
   float2* w;               // divisor work plane of G's projection (partial coherence)
   float2* w2;              // ... of G2's (DM)
+  const float* spec_r;     // energy spectrum: rescale factors, or null
+  const float* spec_w;     // ... and weights
+  float* p;                // squared-divisor plane of G's projection (spectrum)
+  float* p2;               // ... of G2's (DM)
+  int32_t spec_n;          // spectrum samples (0 = none)
+  int32_t pad2_;
 };
 
 struct Item {
@@ -537,14 +543,17 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
 // random-phase start), and does it project (and so want its G tile)?
 // (Projections of partially coherent slots run in the sp_coherence kernels
 // instead; the column pass only builds their random-phase start.)
+__device__ __forceinline__ bool slot_partial(const Slot& s) {
+  return s.ipsf != nullptr || s.spec_n > 0;
+}
 __device__ __forceinline__ bool col_live(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
   return step >= 0 && step <= s.n_iter &&
-         (step > 0 ? s.ipsf == nullptr : s.init == SP_INIT_RANDOM_PHASE);
+         (step > 0 ? !slot_partial(s) : s.init == SP_INIT_RANDOM_PHASE);
 }
 __device__ __forceinline__ bool col_projects(const Slot& s, int tick) {
   const int step = tick - s.start_tick;
-  return step >= 1 && step <= s.n_iter && s.ipsf == nullptr;
+  return step >= 1 && step <= s.n_iter && !slot_partial(s);
 }
 
 // This thread's last-stage butterflies of a column item: butterfly u is row

@@ -74,6 +74,7 @@ class TrialSpec:
     errors: Optional[torch.Tensor] = None  # float64 (iterations, 2) per-iteration sums
     quirks: str = "gpu"
     ipsf: Optional[torch.Tensor] = None    # complex64 (N, N): partially coherent projection
+    spectrum: Optional[tuple] = None       # (rescales, weights) float32 CUDA tensors (n,)
 
     @property
     def n(self):
@@ -116,6 +117,16 @@ def _to_struct(t: TrialSpec) -> _lib.sp_trial:
         if x.dtype != torch.complex64 or tuple(x.shape) != (N, N) or not x.is_cuda or not x.is_contiguous():
             raise ValueError("ipsf must be a contiguous CUDA complex64 tensor of shape (%d, %d)" % (N, N))
         s.ipsf_dev = x.data_ptr()
+    if t.spectrum is not None:
+        r, w = t.spectrum
+        for x in (r, w):
+            if x.dtype != torch.float32 or not x.is_cuda or not x.is_contiguous() or x.dim() != 1:
+                raise ValueError("spectrum must be two contiguous CUDA float32 vectors")
+        if r.numel() != w.numel() or r.numel() == 0:
+            raise ValueError("spectrum rescales and weights must have the same, non-zero length")
+        s.spectrum_rescale_dev = r.data_ptr()
+        s.spectrum_weight_dev = w.data_ptr()
+        s.spectrum_n = r.numel()
     return s
 
 

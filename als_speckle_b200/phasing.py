@@ -12,10 +12,10 @@ Differences from the reference, all deliberate:
   reference's CPU-branch forms instead (``phasing.py:1257``, ``:1284``).
 * Where ``|FFT(psi)| == 0`` the reference divides by zero
   (``phasing_fourier.cl:14``); here the modulus is kept with zero phase.
-* The energy ``spectrum`` (longitudinal coherence, ``radial_rescale``) and
-  ``debug_on`` FITS dumps are not supported and raise.  ``ipsf`` (transverse
-  coherence) is supported; where its blurred divisor is 0 the modulus is kept
-  with zero phase, like the coherent case.
+* ``debug_on`` FITS dumps are not supported and raise.  ``ipsf`` (transverse
+  coherence) and ``spectrum`` (longitudinal coherence, the reference's
+  GPU-only ``radial_rescale``) are supported; where the blurred divisor is 0
+  the modulus is kept with zero phase, like the coherent case.
 """
 from __future__ import annotations
 
@@ -72,8 +72,17 @@ class phasing(common):
         for name, x in (("modulus", modulus), ("support", support), ("ipsf", ipsf)):
             if x is not None and not isinstance(x, np.ndarray):
                 raise TypeError("%s must be ndarray if supplied" % name)
+        # spectrum: (2, n) array of (energies, weights); rescale factors are
+        # energies / the energy of the largest weight (phasing.py:426-450)
         if spectrum is not None:
-            raise NotImplementedError("energy-spectrum (longitudinal coherence) projections are not supported")
+            if not isinstance(spectrum, np.ndarray) or spectrum.ndim != 2 or spectrum.shape[0] != 2:
+                raise ValueError("spectrum must be an ndarray of shape (2, n)")
+            energies, weights = spectrum[0], spectrum[1]
+            rescales = energies / energies[weights.argmax()]
+            self.rescales = torch.from_numpy(rescales.astype(np.float32)).to(self.device)
+            self.sweights = torch.from_numpy(weights.astype(np.float32)).to(self.device)
+            self.N_spctrm = int(energies.shape[0])
+            self.spectrum_state = 2
         if modulus is not None:
             if modulus.ndim != 2:
                 raise ValueError("modulus must be 2d")
@@ -152,6 +161,10 @@ class phasing(common):
         """The loaded ipsf when the projection is partially coherent, else None."""
         return self.ipsf if self.ipsf_state == 2 else None
 
+    def _spectrum(self):
+        """(rescales, weights) on the device when a spectrum is loaded, else None."""
+        return (self.rescales, self.sweights) if self.spectrum_state == 2 else None
+
     # ------------------------------------------------------------------ seed
     def seed(self, val=None, supplied=None):
         """psi_in = (U[0,1) + i U[0,1)) * support from numpy's global RNG, or a
@@ -213,7 +226,8 @@ class phasing(common):
                              iterations=n, order=_runs_from_flat(rot), beta=beta,
                              box=(self.r0, self.c0, self.rows, self.cols) if last else None,
                              save=self.savebuffer[self.numtrial] if last else None,
-                             errors=self.errors[done:done + n], quirks="gpu", ipsf=self._ipsf())
+                             errors=self.errors[done:done + n], quirks="gpu", ipsf=self._ipsf(),
+                             spectrum=self._spectrum())
             self.engine.solve([spec])
             done += n
             if silent is not True and (isinstance(silent, bool) or done % chunk == 0):
@@ -249,7 +263,7 @@ class phasing(common):
                                    box=(self.r0, self.c0, self.rows, self.cols),
                                    save=self.savebuffer[self.numtrial + k],
                                    errors=errs[k] if errors else None, quirks=self.quirks,
-                                   ipsf=self._ipsf()))
+                                   ipsf=self._ipsf(), spectrum=self._spectrum()))
         self.engine.solve(specs)
         self.numtrial += trials
         return (psis, errs) if errors else psis

@@ -80,6 +80,11 @@ typedef struct sp_trial {
                                       corner-centred (phasing.load ipsf=, phasing.py:413-424;
                                       divisor phasing.py:1122-1137), or NULL for a coherent
                                       projection */
+  const float* spectrum_rescale_dev; /* spectrum_n energy / centre-energy rescale factors
+                                        (phasing.py:426-450), for the longitudinal divisor
+                                        phasing.py:1139-1156 and radial_rescale.cl */
+  const float* spectrum_weight_dev;  /* spectrum_n spectral weights */
+  int32_t spectrum_n;                /* samples of the spectrum, 0 = none */
 } sp_trial;
 
 typedef struct sp_run_opts {

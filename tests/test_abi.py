@@ -46,9 +46,10 @@ def test_struct_layout_matches_c(tmp_path):
 #include <stddef.h>
 #include "speckle_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(sp_trial), offsetof(sp_trial, beta),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(sp_trial), offsetof(sp_trial, beta),
          offsetof(sp_trial, psi_dev), offsetof(sp_trial, errors_dev), sizeof(sp_run_opts),
-         offsetof(sp_run_opts, e_per_logn), offsetof(sp_trial, r0), offsetof(sp_trial, ipsf_dev));
+         offsetof(sp_run_opts, e_per_logn), offsetof(sp_trial, r0), offsetof(sp_trial, ipsf_dev),
+         offsetof(sp_trial, spectrum_n));
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -56,7 +57,8 @@ int main(void) {
     vals = [int(v) for v in subprocess.check_output([str(exe)]).split()]
     T, O = _lib.sp_trial, _lib.sp_run_opts
     assert vals == [C.sizeof(T), T.beta.offset, T.psi_dev.offset, T.errors_dev.offset,
-                    C.sizeof(O), O.e_per_logn.offset, T.r0.offset, T.ipsf_dev.offset]
+                    C.sizeof(O), O.e_per_logn.offset, T.r0.offset, T.ipsf_dev.offset,
+                    T.spectrum_n.offset]
 
 
 def test_host_side_errors_without_gpu(lib):
