@@ -106,6 +106,11 @@ _SIGS = {
     "sp_rftf_from_error": ([_p, _p, _i64, _i, _p], _i),
     "sp_remove_hot_pixels": ([_p, _p, _i, _i, _i, _i, _f, _p], _i),
     "sp_covar_pairs": ([_p, _i, _p, _i, _p, _i, _p, _p], _i),
+    "sp_divide_f2_f2": ([_p, _p, _p, _i64, _p], _i),
+    "sp_flip_f2": ([_p, _p, _i, _i, _p], _i),
+    "sp_gaussian": ([_p, _i, _f, _f, _i, _p], _i),
+    "sp_richardson_lucy": ([_p, _p, _p, _p, _p, _i, _i, _i, _p], _i),
+    "sp_coherence_misfit": ([_p, _p, _f, _f, _i, _p, _p, _p], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(lib, _name)

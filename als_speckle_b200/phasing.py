@@ -165,6 +165,98 @@ class phasing(common):
         """(rescales, weights) on the device when a spectrum is loaded, else None."""
         return (self.rescales, self.sweights) if self.spectrum_state == 2 else None
 
+    # ------------------------------------------------------- coherence estimate
+    def optimize_coherence(self, best_estimate, modulus=None, force_cpu=False, load=True,
+                           silent=False, iterations=500, method="richardson_lucy",
+                           is_fourier=False):
+        """Estimate the coherence function from reconstructions
+        (``phasing.py:507-930``).
+
+        ``richardson_lucy``: for every frame at once, Richardson-Lucy
+        deconvolution of the measured intensity M^2 by the frame's intensity
+        (``iterations`` steps from a Gaussian of width N/4); the result is the
+        last frame's transform divided by its value at (0,0), as in the
+        reference (its sum over frames is unused), loaded as the ipsf if
+        ``load`` and returned fftshifted.  ``gaussian``: per frame, the
+        coherence lengths minimising the misfit between the modulus and the
+        speckle of the damped autocorrelation (``scipy.optimize.fmin`` on the
+        host, each evaluation on the device); their mean loads a Gaussian
+        ipsf if ``load``; returns the (2, frames) lengths.  ``force_cpu``
+        raises (no CPU branch)."""
+        if force_cpu:
+            raise NotImplementedError("als_speckle_b200 has no CPU branch")
+        if method not in ("richardson_lucy", "gaussian"):
+            raise ValueError("unknown coherence method %s" % method)
+        if modulus is None:
+            if self.modulus is None:
+                raise RuntimeError("no modulus: load one or pass modulus=")
+            modulus = self.modulus.cpu().numpy()
+        modulus = np.asarray(modulus)
+        if modulus.ndim != 2 or modulus.shape[0] != modulus.shape[1]:
+            raise ValueError("modulus must be square 2d")
+        N = modulus.shape[0]
+        est = best_estimate.cpu().numpy() if isinstance(best_estimate, torch.Tensor) else np.asarray(best_estimate)
+        if est.ndim == 2:
+            est = est[None]
+        if est.ndim != 3 or est.shape[1] > N or est.shape[2] > N:
+            raise ValueError("best_estimate must be 2d or 3d and no larger than the modulus")
+        F = est.shape[0]
+        dev = self.device
+        st = stream_ptr()
+        active = torch.zeros((F, N, N), dtype=torch.complex64, device=dev)
+        active[:, :est.shape[1], :est.shape[2]] = torch.from_numpy(est.astype(np.complex64)).to(dev)
+        if method == "richardson_lucy":
+            # p = |FFT(estimate)|^2 / sum (the estimate is already a modulus if
+            # is_fourier), P = FFT(p), PH = P flipped; d = M^2 / sum
+            p = active.clone()
+            if not is_fourier:
+                call("sp_fft2", ptr(p), ptr(p), N, F, 0, st)
+                call("sp_abs_f2_f2", ptr(p), ptr(p), p.numel(), st)
+            call("sp_multiply_f2_f2", ptr(p), ptr(p), ptr(p), p.numel(), st)
+            sums = p.real.sum(dim=(1, 2), dtype=torch.float64)
+            p.mul_((1.0 / sums).to(torch.float32).view(F, 1, 1))
+            call("sp_fft2", ptr(p), ptr(p), N, F, 0, st)
+            ph = torch.empty_like(p)
+            call("sp_flip_f2", ptr(p), ptr(ph), N, F, st)
+            m2 = modulus.astype(np.float64) ** 2
+            d = torch.from_numpy((m2 / m2.sum()).astype(np.complex64)).to(dev)
+            u = torch.empty((F, N, N), dtype=torch.complex64, device=dev)
+            call("sp_gaussian", ptr(u[0]), N, C.c_float(N / 4.0), C.c_float(N / 4.0), 1, st)
+            u[1:] = u[0]
+            work = torch.empty_like(u)
+            call("sp_richardson_lucy", ptr(u), ptr(p), ptr(ph), ptr(d), ptr(work), N, F,
+                 int(iterations), st)
+            last = u[F - 1].contiguous()
+            call("sp_fft2", ptr(last), ptr(last), N, 1, 0, st)
+            ipsf = last.cpu().numpy()
+            ipsf = (ipsf * (1.0 / abs(ipsf[0, 0]))).astype(np.complex64)
+            if load:
+                self.load(ipsf=ipsf)
+            return np.fft.fftshift(ipsf)
+        # gaussian: autocorrelation IFFT(|FFT(estimate)|^2) per frame, then fmin
+        from scipy.optimize import fmin
+        call("sp_fft2", ptr(active), ptr(active), N, F, 0, st)
+        call("sp_abs2_f2_f2", ptr(active), ptr(active), active.numel(), st)
+        call("sp_fft2", ptr(active), ptr(active), N, F, 1, st)
+        m = torch.from_numpy(np.ascontiguousarray(modulus, np.float32)).to(dev)
+        work = torch.empty((N, N), dtype=torch.complex64, device=dev)
+        acc = torch.empty(1, dtype=torch.float64, device=dev)
+        optcls = np.zeros((2, F), np.float32)
+        for n in range(F):
+            ac = active[n]
+
+            def misfit(cl):
+                call("sp_coherence_misfit", ptr(ac), ptr(m), C.c_float(cl[0]), C.c_float(cl[1]), N,
+                     ptr(work), ptr(acc), st)
+                return float(acc.item())
+            optcls[:, n] = fmin(misfit, (N / 2, N / 2), disp=False, ftol=.1, xtol=0.1)
+        ave = np.average(optcls, axis=1)
+        if load:
+            rows, cols = np.indices((N, N)) - N / 2.
+            rows, cols = np.fft.fftshift(rows), np.fft.fftshift(cols)
+            self.load(ipsf=np.exp(-rows ** 2 / (2 * ave[0] ** 2)) * np.exp(-cols ** 2 / (2 * ave[1] ** 2)))
+        return optcls
+
     # ------------------------------------------------------------------ seed
     def seed(self, val=None, supplied=None):
         """psi_in = (U[0,1) + i U[0,1)) * support from numpy's global RNG, or a

@@ -1,6 +1,6 @@
 """The benchmark workloads other than the headline batched HIO job.
 
-    python -m als_speckle_b200.workloads single256 | raar_dm1024 | uneven | serving | coherence512 [--out f.json]
+    python -m als_speckle_b200.workloads single256 | raar_dm1024 | uneven | serving | coherence512 | quality [--out f.json]
 
 * ``single256``   one 256^2 trial, 200 HIO (beta 0.9) + 20 ER, random-phase start,
                    through ``phasing.iterate_trials``; final R-factor.
@@ -12,9 +12,13 @@
                    engine call versus one call per trial.
 * ``serving``     Poisson request stream through the continuous-batching
                    service; p50 / p99 latency, throughput, sustainable rate.
-* ``coherence512`` 32 x 512^2 trials, 200 HIO (beta 0.9), random-phase starts,
-                   with a partially coherent projection (Gaussian point spread,
-                   sigma 2 px) and without; trial-iterations/s of both.
+* ``coherence512`` 32 x 512^2 trials, 200 HIO (beta 0.9), random-phase starts:
+                   coherent, with an ipsf (Gaussian point spread, sigma 2 px),
+                   with an energy spectrum (7 samples, +-5%), and with both;
+                   trial-iterations/s of each.
+* ``quality``     128 reconstructions (180^2 crops of one object plus noise):
+                   gpu_rftf against a 512^2 goal, rftf of their average, and
+                   covar_results over all 8256 pairs (256^2 transforms).
 
 All inputs are seeded synthetic patterns (``synth``); results are printed as
 one JSON object.
@@ -194,10 +198,15 @@ def coherence512(trials=32, iters=200, seed=0):
     eng = Engine(device=dev, use_graph=True, e_per_n={N: autotune.load_or_default(N)["E"]})
     stream = torch.cuda.Stream()
     out = {"workload": "coherence512", "trials": trials, "iterations": iters}
-    for name, ip in (("coherent", None), ("partially_coherent", ipsf)):
+    e = np.linspace(0.95, 1.05, 7)
+    w = np.exp(-0.5 * np.linspace(-2, 2, 7) ** 2)
+    spec = (torch.from_numpy((e / e[3]).astype(np.float32)).to(dev),
+            torch.from_numpy(w.astype(np.float32)).to(dev))
+    for name, ip, sp in (("coherent", None, None), ("partially_coherent", ipsf, None),
+                         ("spectrum", None, spec), ("ipsf_and_spectrum", ipsf, spec)):
         specs = [TrialSpec(psi=psis[k], modulus=Md, support=Sd, iterations=iters,
                            order=(("hio", iters),), beta=0.9, random_phase=True, seed=seed,
-                           trial=k, ipsf=ip) for k in range(trials)]
+                           trial=k, ipsf=ip, spectrum=sp) for k in range(trials)]
         with torch.cuda.stream(stream):
             eng.solve(specs, stream=stream)  # warm-up (graph capture)
             stream.synchronize()
@@ -208,9 +217,36 @@ def coherence512(trials=32, iters=200, seed=0):
     return out
 
 
+def quality(frames=128, seed=0):
+    """Trial-quality measures on a batch of reconstructions."""
+    from .phasing import gpu_rftf, rftf, covar_results
+    rng = np.random.default_rng(seed)
+    obj, M, _ = synth.config_pattern("hio_512x128", seed=seed)
+    crop = obj[166:346, 166:346]
+    recs = (crop[None] * np.exp(1j * rng.uniform(-np.pi, np.pi, (frames, 1, 1)))
+            + 0.05 * (rng.standard_normal((frames, 180, 180)) + 1j * rng.standard_normal((frames, 180, 180))))
+    recs = recs.astype(np.complex64)
+    dev = torch.device("cuda")
+    recs_d = torch.from_numpy(recs).to(dev)
+    Md = torch.from_numpy(M).to(dev)
+    gpu_rftf(None, recs_d[:2], Md)  # warm-up
+    _, t_gr = _timed(lambda: gpu_rftf(None, recs_d, Md))
+    avg = recs_d.mean(0)
+    rftf(avg, Md)
+    _, t_r = _timed(lambda: rftf(avg, Md))
+    covar_results(None, recs[:4], threshold=0.9)
+    (cc, cov, stats, _), t_c = _timed(lambda: covar_results(None, recs, threshold=0.9))
+    pairs = frames * (frames + 1) // 2
+    return {"workload": "quality", "frames": frames, "gpu_rftf_seconds": t_gr,
+            "rftf_seconds": t_r, "covar_results_seconds": t_c, "covar_pairs": pairs,
+            "covar_pairs_per_s": pairs / t_c, "covar_transform": 256,
+            "mean_covariance": float(cov.mean())}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=("single256", "raar_dm1024", "uneven", "serving", "coherence512"))
+    ap.add_argument("workload", choices=("single256", "raar_dm1024", "uneven", "serving", "coherence512",
+                                         "quality"))
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--window", type=float, default=0.5)
     ap.add_argument("--rounds", type=int, default=None)
@@ -225,6 +261,8 @@ def main():
         r = uneven(iters=a.iters)
     elif a.workload == "coherence512":
         r = coherence512()
+    elif a.workload == "quality":
+        r = quality()
     else:
         r = serving(rate=a.rate, window=a.window)
     line = json.dumps(r)

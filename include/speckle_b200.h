@@ -250,6 +250,26 @@ int sp_remove_hot_pixels(float* data_dev, float* work_dev, int frames, int rows,
 int sp_covar_pairs(const void* dfts_dev, int N, const int32_t* pairs_dev, int n_pairs,
                    void* work_dev, int work_planes, float* cc_dev, sp_stream_t stream);
 
+/* ---- coherence estimation (phasing.optimize_coherence, phasing.py:507-930) */
+/* out = in1 / in2, complex  -- kernels/common_divide_f2_f2.cl */
+int sp_divide_f2_f2(const void* in1_dev, const void* in2_dev, void* out_dev, int64_t n,
+                    sp_stream_t stream);
+/* out[N-1-i][N-1-j] = in[i][j] for each of `planes` N*N planes (in != out)
+ * -- kernels/common_flip_f2.cl */
+int sp_flip_f2(const void* in_dev, void* out_dev, int N, int planes, sp_stream_t stream);
+/* exp(-i^2/(2 sx^2)) exp(-j^2/(2 sy^2)) in corner-centred coordinates, N*N floats, or
+ * complex64 with zero imaginary part if complex_out  -- kernels/common_gaussian_f.cl */
+int sp_gaussian(void* out_dev, int N, float sx, float sy, int complex_out, sp_stream_t stream);
+/* `iterations` Richardson-Lucy steps for `frames` estimates u at once (_opt_iter_rl,
+ * phasing.py:702-738): blur = IFFT(FFT(u) p_hat); blur = d / blur; blur = IFFT(FFT(blur)
+ * ph_hat); u *= blur.  p_hat, ph_hat, u, work: frames*N*N complex64; d: N*N complex64. */
+int sp_richardson_lucy(void* u_dev, const void* p_hat_dev, const void* ph_hat_dev, const void* d_dev,
+                       void* work_dev, int N, int frames, int iterations, sp_stream_t stream);
+/* the Gaussian fit's objective (_opt_iter_g, phasing.py:663-700): *sum_dev (FP64) =
+ * sum (sqrt|FFT2(gaussian(sx, sy) * ac)| - modulus)^2; work_dev: N*N complex64. */
+int sp_coherence_misfit(const void* ac_dev, const float* modulus_dev, float sx, float sy, int N,
+                        void* work_dev, double* sum_dev, sp_stream_t stream);
+
 /* ---- plain single-instance path (the reference's GPU dataflow) --------- */
 /* One trial, cuFFT C2C plans plus one elementwise kernel per step with a
  * stream synchronisation after each, as phasing.py:1187-1353 drives pyfft and

@@ -222,6 +222,34 @@ def quality():
     np.savez_compressed(os.path.join(HERE, "quality.npz"), **out)
 
 
+def coherence_opt():
+    """optimize_coherence (phasing.py:507-930), numpy branch: Richardson-Lucy
+    on one frame (the branch fails on a second) and the Gaussian fit on two."""
+    import warnings
+    out = {}
+    N, B = 32, 10
+    rng = np.random.default_rng(9)
+    obj = np.zeros((N, N), np.complex128)
+    obj[11:11 + B, 11:11 + B] = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.5, 0.5, (B, B)))
+    blur = gaussian_ipsf(N, 1.2)
+    M = np.sqrt(np.abs(np.fft.ifft2(np.fft.fft2(np.abs(np.fft.fft2(obj)) ** 2) * blur))).astype(np.float32)
+    est1 = obj[8:24, 8:24].astype(np.complex64)[None]
+    est2 = np.stack([obj[8:24, 8:24], obj[8:24, 8:24] * 0.9 + 0.01]).astype(np.complex64)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+        rl = _quiet(r.optimize_coherence, est1.copy(), modulus=M, force_cpu=True, load=False,
+                    silent=True, iterations=6, method="richardson_lucy")
+        r2 = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+        cl = _quiet(r2.optimize_coherence, est2.copy(), modulus=M, force_cpu=True, load=False,
+                    silent=True, method="gaussian")
+    out["modulus"], out["est1"], out["est2"] = M, est1, est2
+    out["rl_iterations"] = np.int64(6)
+    out["rl_ipsf"] = np.asarray(rl)
+    out["gaussian_lengths"] = np.asarray(cl)
+    np.savez_compressed(os.path.join(HERE, "coherence_opt.npz"), **out)
+
+
 if __name__ == "__main__":
     projections()
     trajectories()
@@ -229,6 +257,7 @@ if __name__ == "__main__":
     helpers()
     coherence()
     quality()
+    coherence_opt()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -140,3 +140,44 @@ def test_phasing_class_with_ipsf(coh):
     r.iterate(3, order=(("hio", 2), ("raar", 1)), beta=0.9)
     want = O.iterate(psi0, M, S, 3, order=(("hio", 2), ("raar", 1)), beta=0.9, mode="f64", ipsf=ip)
     assert rel(r.get(r.psi_in), want) < 1e-4
+
+
+# ------------------------------------------------ optimize_coherence
+@pytest.fixture(scope="module")
+def copt():
+    return np.load(os.path.join(G, "coherence_opt.npz"))
+
+
+def test_optimize_coherence_rl_vs_reference_golden(copt):
+    """Richardson-Lucy on one frame: the reference's numpy branch keeps the
+    real part of the (complex) estimate; compare that part to 1e-4."""
+    from als_speckle_b200.phasing import phasing
+    r = phasing()
+    out = r.optimize_coherence(copt["est1"], modulus=copt["modulus"], load=False, silent=True,
+                               iterations=int(copt["rl_iterations"]))
+    want = copt["rl_ipsf"]
+    assert np.linalg.norm(out.real - want) / np.linalg.norm(want) < 1e-4
+
+
+def test_optimize_coherence_rl_frames_are_independent(copt):
+    """Batched over frames, the result (the last frame's estimate) equals the
+    last frame run alone, and loading it sets the ipsf."""
+    from als_speckle_b200.phasing import phasing
+    r = phasing()
+    M = copt["modulus"]
+    both = r.optimize_coherence(copt["est2"], modulus=M, load=True, silent=True, iterations=5)
+    assert r.ipsf_state == 1  # no modulus loaded yet: waiting for it
+    alone = r.optimize_coherence(copt["est2"][1:], modulus=M, load=False, silent=True, iterations=5)
+    assert np.array_equal(both, alone)
+    assert abs(abs(np.fft.ifftshift(both)[0, 0]) - 1) < 1e-6  # divided by its magnitude there
+
+
+def test_optimize_coherence_gaussian_vs_reference_golden(copt):
+    """Gaussian fit: lengths agree with the reference's to the optimiser's
+    own tolerance (xtol 0.1); the objective runs on the device."""
+    from als_speckle_b200.phasing import phasing
+    r = phasing()
+    out = r.optimize_coherence(copt["est2"], modulus=copt["modulus"], load=False, silent=True,
+                               method="gaussian")
+    assert out.shape == (2, 2)
+    assert np.max(np.abs(out - copt["gaussian_lengths"])) < 0.15
