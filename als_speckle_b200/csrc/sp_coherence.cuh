@@ -251,44 +251,107 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b1_kernel(PcArgs a) {
 // coordinates (x = i or i - N for column i, y likewise for row j); taps at
 // or beyond -N/2 and N/2 carry weight 0 and are not read (the reference
 // reads them, possibly outside the array, and multiplies by 0).
+// The bilinear taps are separable: column i's two source columns and their
+// weights depend only on (k, i), row j's only on (k, j).  A block takes a
+// tile of TC columns x RB rows; each thread owns one column and RT of the
+// tile's rows.  The row taps of up to RQ samples are built once per tile in
+// shared memory, a thread's column taps in registers, so each sample costs a
+// pixel four loads and a few FMAs; the per-pixel arithmetic is the kernel's
+// own (same order of terms).
+struct RescaleTap {
+  int i1, i2;    // source index of each tap (column, or row * N); -1 = weight 0, not read
+  float w1, w2;  // 1 - |tap - r|
+};
+
+// pixels of one rescale tile (TC columns x RB rows, below), for grid sizing
+__host__ __device__ constexpr int rescale_tile_pixels(int N) {
+  return (N < kThreads ? N : kThreads) *
+         (N < 8 * (kThreads / (N < kThreads ? N : kThreads)) ? N : 8 * (kThreads / (N < kThreads ? N : kThreads)));
+}
+
 template <int N>
-__global__ void __launch_bounds__(kThreads) pc_rescale_kernel(PcArgs a) {
+struct RescaleTile {
+  static constexpr int TC = N < kThreads ? N : kThreads;  // columns, one per thread
+  static constexpr int G = kThreads / TC;                 // row groups
+  static constexpr int RB = N < 8 * G ? N : 8 * G;         // rows per tile
+  static constexpr int RT = (RB + G - 1) / G;              // rows per thread
+  static constexpr int RQ = 16;                            // samples per table fill
+  static_assert(TC * RB == rescale_tile_pixels(N), "tile size");
+};
+
+// taps of coordinate c (corner-centred) at rescale r; `stride` scales the index
+__device__ __forceinline__ RescaleTap rescale_tap(int N, float c, float r, int stride) {
+  const int N2 = N / 2;
+  const float rc = c / r;
+  const int c1 = (int)floorf(rc), c2 = c1 + 1;
+  const bool k1 = c1 > -N2 && c1 < N2, k2 = c2 > -N2 && c2 < N2;
+  RescaleTap t;
+  t.w1 = k1 ? 1.f - fabsf((float)c1 - rc) : 0.f;
+  t.w2 = k2 ? 1.f - fabsf((float)c2 - rc) : 0.f;
+  t.i1 = k1 ? (c1 < 0 ? c1 + N : c1) * stride : -1;
+  t.i2 = k2 ? (c2 < 0 ? c2 + N : c2) * stride : -1;
+  return t;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kThreads, 6) pc_rescale_kernel(PcArgs a) {
+  using RT_ = RescaleTile<N>;
+  constexpr int TC = RT_::TC, G = RT_::G, RB = RT_::RB, RT = RT_::RT, RQ = RT_::RQ;
   constexpr int N2 = N / 2;
-  constexpr int64_t PLANE = (int64_t)N * N;
-  for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < a.n_jobs * PLANE;
-       it += (int64_t)gridDim.x * blockDim.x) {
-    const int j = (int)(it / PLANE);
-    const int64_t k = it - (int64_t)j * PLANE;
+  constexpr int TILES = (N / TC) * (N / RB);
+  __shared__ RescaleTap yt[RQ][RB];
+  __shared__ float rq[RQ], wq[RQ];
+  const int tc = threadIdx.x % TC, g = threadIdx.x / TC;
+  for (int it = blockIdx.x; it < a.n_jobs * TILES; it += gridDim.x) {
+    const int j = it / TILES, tile = it - j * TILES;
     const int2 job = a.jobs[j];
     const Slot& s = a.slots[job.x];
-    if (!pc_active(s, job.y, a.tick) || s.spec_n == 0) continue;
-    const float* pp = job.y ? s.p2 : s.p;
+    if (!pc_active(s, job.y, a.tick) || s.spec_n == 0) continue;  // uniform over the block
+    const float* __restrict__ pp = job.y ? s.p2 : s.p;
     float* out = reinterpret_cast<float*>(job.y ? s.w2 : s.w);
-    const int row = (int)(k / N), col = (int)(k - (int64_t)row * N);
-    const float x = (float)(col > N2 - 1 ? col - N : col);
-    const float y = (float)(row > N2 - 1 ? row - N : row);
-    float cum = 0.f;
-    for (int q = 0; q < s.spec_n; ++q) {
-      const float rv = s.spec_r[q], sw = s.spec_w[q];
-      const float rx = x / rv, ry = y / rv;
-      const int x1 = (int)floorf(rx), y1 = (int)floorf(ry);
-      const int x2 = x1 + 1, y2 = y1 + 1;
-      const bool kx1 = x1 > -N2 && x1 < N2, kx2 = x2 > -N2 && x2 < N2;
-      const bool ky1 = y1 > -N2 && y1 < N2, ky2 = y2 > -N2 && y2 < N2;
-      const float wx1 = kx1 ? 1.f - fabsf((float)x1 - rx) : 0.f;
-      const float wx2 = kx2 ? 1.f - fabsf((float)x2 - rx) : 0.f;
-      const float wy1 = ky1 ? 1.f - fabsf((float)y1 - ry) : 0.f;
-      const float wy2 = ky2 ? 1.f - fabsf((float)y2 - ry) : 0.f;
-      const int c1 = x1 < 0 ? x1 + N : x1, c2 = x2 < 0 ? x2 + N : x2;
-      const int r1 = y1 < 0 ? y1 + N : y1, r2 = y2 < 0 ? y2 + N : y2;
-      const float v11 = (kx1 && ky1) ? pp[(int64_t)r1 * N + c1] : 0.f;
-      const float v12 = (kx1 && ky2) ? pp[(int64_t)r2 * N + c1] : 0.f;
-      const float v21 = (kx2 && ky1) ? pp[(int64_t)r1 * N + c2] : 0.f;
-      const float v22 = (kx2 && ky2) ? pp[(int64_t)r2 * N + c2] : 0.f;
-      const float iv = v11 * wx1 * wy1 + v12 * wx1 * wy2 + v21 * wx2 * wy1 + v22 * wx2 * wy2;
-      cum += iv * sw;
+    const int c0 = (tile % (N / TC)) * TC, r0 = (tile / (N / TC)) * RB;
+    const int col = c0 + tc;
+    const float xc = (float)(col > N2 - 1 ? col - N : col);
+    float cum[RT];
+#pragma unroll
+    for (int u = 0; u < RT; ++u) cum[u] = 0.f;
+    for (int q0 = 0; q0 < s.spec_n; q0 += RQ) {
+      const int nq = s.spec_n - q0 < RQ ? s.spec_n - q0 : RQ;
+      __syncthreads();  // the previous tile or sample group is done with the tables
+      for (int e = threadIdx.x; e < nq * RB; e += kThreads) {
+        const int q = e / RB, r = r0 + e % RB;
+        yt[q][e % RB] = rescale_tap(N, (float)(r > N2 - 1 ? r - N : r), s.spec_r[q0 + q], N);
+      }
+      if (threadIdx.x < nq) {
+        rq[threadIdx.x] = s.spec_r[q0 + threadIdx.x];
+        wq[threadIdx.x] = s.spec_w[q0 + threadIdx.x];
+      }
+      __syncthreads();
+#pragma unroll 2
+      for (int q = 0; q < nq; ++q) {
+        const RescaleTap x = rescale_tap(N, xc, rq[q], 1);
+        const float sw = wq[q];
+#pragma unroll
+        for (int u = 0; u < RT; ++u) {
+          const int lr = g + u * G;
+          if (RB % G == 0 || lr < RB) {
+            const RescaleTap y = yt[q][lr];
+            const float v11 = (x.i1 >= 0 && y.i1 >= 0) ? pp[y.i1 + x.i1] : 0.f;
+            const float v12 = (x.i1 >= 0 && y.i2 >= 0) ? pp[y.i2 + x.i1] : 0.f;
+            const float v21 = (x.i2 >= 0 && y.i1 >= 0) ? pp[y.i1 + x.i2] : 0.f;
+            const float v22 = (x.i2 >= 0 && y.i2 >= 0) ? pp[y.i2 + x.i2] : 0.f;
+            const float iv = v11 * x.w1 * y.w1 + v12 * x.w1 * y.w2 + v21 * x.w2 * y.w1 +
+                             v22 * x.w2 * y.w2;
+            cum[u] += iv * sw;
+          }
+        }
+      }
     }
-    out[k] = cum;
+#pragma unroll
+    for (int u = 0; u < RT; ++u) {
+      const int lr = g + u * G;
+      if (RB % G == 0 || lr < RB) out[(int64_t)(r0 + lr) * N + col] = cum[u];
+    }
   }
 }
 

@@ -305,7 +305,9 @@ static cudaError_t launch_transpose(const float* src, float* dst, int N, cudaStr
 struct Segment {
   int N, E, first, count, grid[2];  // grid[pass]: 0 column, 1 row
   int pc_first, pc_count, pc_grid;  // partial-coherence jobs of this size
-  int pc_egrid;                     // grid of the elementwise rescale kernel
+  int pc_egrid;                     // grid of the tiled rescale kernel
+  int col_ticks;                    // the column pass runs at ticks [0, col_ticks)
+  int pc_mask;                      // partial-coherence kernels launched (bit = which)
 };
 
 struct GraphKey {
@@ -329,10 +331,12 @@ static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, con
       if (sg.pc_count == 0) continue;
       PcArgs pa{slots, jobs + sg.pc_first, sg.pc_count, k, tw};
       for (int which = 0; which < 5; ++which)
-        SP_CUDA_TRY(launch_pc(sg.N, which, which == 3 ? sg.pc_egrid : sg.pc_grid, st, pa));
+        if (sg.pc_mask & (1 << which))
+          SP_CUDA_TRY(launch_pc(sg.N, which, which == 3 ? sg.pc_egrid : sg.pc_grid, st, pa));
     }
     for (int which = 0; which < 2; ++which) {
       for (const Segment& sg : segs) {
+        if (which == 0 && k >= sg.col_ticks) continue;  // no column work left in this segment
         // the column pass walks the items backwards: it starts on the
         // trials whose G planes the row pass wrote last (still in L2), and
         // the next row pass starts on the ones it wrote last
@@ -415,7 +419,15 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       if (count == 0) continue;
       int occ[2] = {1, 1}, sms = 1;
       SP_CUDA_TRY(occupancy_for(N, E, occ, &sms));
-      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1, 1};
+      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1, 1, 0, 0};
+      // Partially coherent slots project in their own kernels: the column
+      // pass has work for them only at tick 0, to start a random phase.  A
+      // segment of such slots alone launches it only while it has work.
+      for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
+        if (trials[i].n != N) continue;
+        if (!partial(trials[i])) sg.col_ticks = INT32_MAX;
+        else if (trials[i].init == SP_INIT_RANDOM_PHASE) sg.col_ticks = std::max(sg.col_ticks, 1);
+      }
       for (int p = 0; p < 2; ++p) {
         int per_sm = occ[p];
         if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
@@ -427,12 +439,18 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
         if (uses_dm(trials[i])) hj.push_back(int2{i, 1});
       }
       sg.pc_count = (int)hj.size() - sg.pc_first;
+      // A and B always; W with an ipsf; R with a spectrum; B1 with both
+      for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
+        if (trials[i].n != N || !partial(trials[i])) continue;
+        const bool ip = trials[i].ipsf_dev != nullptr, sp = trials[i].spectrum_n > 0;
+        sg.pc_mask |= 1 | 16 | (ip ? 2 : 0) | (sp ? 8 : 0) | (ip && sp ? 4 : 0);
+      }
       if (sg.pc_count > 0) {
         SP_CUDA_TRY(pc_ready(N));
         const int per_job = N / lines_per_item(N, pc_e(N));
         sg.pc_grid = std::max(1, std::min(sg.pc_count * per_job, sms * 4));
-        const int64_t ew = ((int64_t)sg.pc_count * N * N + 255) / 256;
-        sg.pc_egrid = (int)std::max<int64_t>(1, std::min<int64_t>(ew, (int64_t)sms * 16));
+        const int64_t tiles = (int64_t)sg.pc_count * N * N / rescale_tile_pixels(N);
+        sg.pc_egrid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sms * 8));
       }
       segs[g].push_back(sg);
     }
@@ -506,9 +524,10 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
   const bool use_graph = opts && opts->use_graph && st != nullptr;
   g_last_launches = (int64_t)L.mt_first.size();
   for (int g = 0; g < n_groups; ++g) {
-    g_last_launches += 2LL * ticks[g] * (int64_t)segs[g].size();
-    for (const Segment& sg : segs[g])
-      if (sg.pc_count) g_last_launches += 5LL * ticks[g];
+    for (const Segment& sg : segs[g]) {
+      g_last_launches += ticks[g] + std::min(ticks[g], sg.col_ticks);
+      g_last_launches += (int64_t)__builtin_popcount(sg.pc_mask) * ticks[g];
+    }
   }
 
   for (int g = 0; g < n_groups; ++g) {
@@ -520,7 +539,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     GraphKey key{workspace_dev, dev, g, ticks[g], {}};
     for (const Segment& sg : segs[g])
       key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1],
-                                         sg.pc_first, sg.pc_count, sg.pc_grid, sg.pc_egrid});
+                                         sg.pc_first, sg.pc_count, sg.pc_grid, sg.pc_egrid,
+                                         std::min(ticks[g], sg.col_ticks), sg.pc_mask});
     cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);
