@@ -48,7 +48,7 @@ __host__ __device__ constexpr int pc_smem_elems() {
 
 // A: F = FFT_cols(G) over G, W = FFT_cols(|F|^2).
 template <int N>
-__global__ void __launch_bounds__(kThreads) pc_cols_a_kernel(PcArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) pc_cols_a_kernel(PcArgs a) {
   constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
   extern __shared__ float2 smem[];
   float2* tw = smem + item_smem_elems(N, E);
@@ -137,10 +137,9 @@ __global__ void __launch_bounds__(kThreads) pc_rows_w_kernel(PcArgs a) {
 // B: divisor from W, projection of F (stored in G), inverse column transform;
 // FP64 error sums of |F| - M for plane 0, one atomic pair per warp.
 template <int N>
-__global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) pc_cols_b_kernel(PcArgs a) {
   constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
   constexpr float inv = 1.0f / ((float)N * (float)N);
-  constexpr float inv_n = 1.0f / (float)N;
   extern __shared__ float2 smem[];
   float2* tw = smem + item_smem_elems(N, E);
   build_stage_twiddles<N, E>(tw, a.tw + N);
@@ -171,23 +170,32 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
     }
     float f2 = 0.f, f1 = 0.f;
     if (active) {
+      // rdv = 1 / divisor (0 where the divisor is 0), from the reciprocal
+      // square root: the divisor is sqrt(D) with D the squared divisor
       if (spec) {  // R left the rescaled squared divisor in W, read as floats
         const float* wf = reinterpret_cast<const float*>(w);
 #pragma unroll
-        for (int i = 0; i < E; ++i) dv[i] = sqrtf(wf[off + (size_t)i * T * N]);
-      } else {
+        for (int i = 0; i < E; ++i) {
+          const float d2 = wf[off + (size_t)i * T * N];
+          dv[i] = d2 > 0.f ? rsqrtf(d2) : 0.f;
+        }
+      } else {  // D = |IFFT_cols(W)| / N^2
 #pragma unroll
-        for (int i = 0; i < E; ++i) dv[i] = sqrtf(sqrtf(v[i].x * v[i].x + v[i].y * v[i].y)) * inv_n;
+        for (int i = 0; i < E; ++i) {
+          const float p2 = v[i].x * v[i].x + v[i].y * v[i].y;
+          dv[i] = p2 > 0.f ? rsqrtf(p2 * rsqrtf(p2)) * (float)N : 0.f;
+        }
       }
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const float2 f = g[off + (size_t)i * T * N];
         const float m = s.modulus[off + (size_t)i * T * N];
-        const float d = sqrtf(f.x * f.x + f.y * f.y) - m;
+        const float p2 = f.x * f.x + f.y * f.y;
+        const float d = (p2 > 0.f ? p2 * rsqrtf(p2) : 0.f) - m;
         f2 = fmaf(d, d, f2);
         f1 += fabsf(d);
         // the reference divides by a zero divisor; keep M with zero phase there
-        const float sc = dv[i] > 0.f ? m / dv[i] * inv : 0.f;
+        const float sc = m * dv[i] * inv;
         v[i] = dv[i] > 0.f ? make_float2(f.x * sc, f.y * -sc) : make_float2(m * inv, 0.f);
       }
     }
@@ -214,7 +222,7 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b_kernel(PcArgs a) {
 // B1: P = |IFFT_cols(W)| / N^2, the squared ipsf divisor, for slots that
 // also have a spectrum.
 template <int N>
-__global__ void __launch_bounds__(kThreads) pc_cols_b1_kernel(PcArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) pc_cols_b1_kernel(PcArgs a) {
   constexpr int E = pc_e(N), T = N / E, C = lines_per_item(N, E);
   constexpr float inv = 1.0f / ((float)N * (float)N);
   extern __shared__ float2 smem[];
@@ -241,7 +249,10 @@ __global__ void __launch_bounds__(kThreads) pc_cols_b1_kernel(PcArgs a) {
     fft_line<N, E, +1>(v, lay, BlockSync{}, active, t, tw);
     if (active) {
 #pragma unroll
-      for (int i = 0; i < E; ++i) pp[off + (size_t)i * T * N] = sqrtf(v[i].x * v[i].x + v[i].y * v[i].y) * inv;
+      for (int i = 0; i < E; ++i) {
+        const float p2 = v[i].x * v[i].x + v[i].y * v[i].y;
+        pp[off + (size_t)i * T * N] = (p2 > 0.f ? p2 * rsqrtf(p2) : 0.f) * inv;
+      }
     }
   }
 }
