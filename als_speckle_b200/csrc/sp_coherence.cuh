@@ -260,18 +260,19 @@ __global__ void __launch_bounds__(kThreads, 4) pc_cols_b1_kernel(PcArgs a) {
 // R: W (read as N*N floats) = radial_rescale(P)  -- phasing_radial_rescale.cl:
 // out(x, y) = sum_k w_k * bilinear(P, x / r_k, y / r_k) with corner-centred
 // coordinates (x = i or i - N for column i, y likewise for row j); taps at
-// or beyond -N/2 and N/2 carry weight 0 and are not read (the reference
-// reads them, possibly outside the array, and multiplies by 0).
+// or beyond -N/2 and N/2 carry weight 0 (the reference reads them, possibly
+// outside the array, and multiplies by 0; here they read an element inside
+// the plane instead, times 0).
 // The bilinear taps are separable: column i's two source columns and their
 // weights depend only on (k, i), row j's only on (k, j).  A block takes a
 // tile of TC columns x RB rows; each thread owns one column and RT of the
-// tile's rows.  The row taps of up to RQ samples are built once per tile in
-// shared memory, a thread's column taps in registers, so each sample costs a
-// pixel four loads and a few FMAs; the per-pixel arithmetic is the kernel's
-// own (same order of terms).
+// tile's rows.  The row taps of up to RQ samples (their weights times w_k)
+// are built once per tile in shared memory, a thread's column taps in
+// registers, so a sample costs a pixel four loads and four FMAs:
+//   out += (w_k wy1) (v11 wx1 + v21 wx2) + (w_k wy2) (v12 wx1 + v22 wx2).
 struct RescaleTap {
-  int i1, i2;    // source index of each tap (column, or row * N); -1 = weight 0, not read
-  float w1, w2;  // 1 - |tap - r|
+  int i1, i2;    // source index of each tap (column, or row * N); 0 where the weight is 0
+  float w1, w2;  // 1 - |tap - r| (times the spectral weight for rows)
 };
 
 // pixels of one rescale tile (TC columns x RB rows, below), for grid sizing
@@ -290,28 +291,29 @@ struct RescaleTile {
   static_assert(TC * RB == rescale_tile_pixels(N), "tile size");
 };
 
-// taps of coordinate c (corner-centred) at rescale r; `stride` scales the index
-__device__ __forceinline__ RescaleTap rescale_tap(int N, float c, float r, int stride) {
+// taps of coordinate c (corner-centred) at rescale r; `stride` scales the
+// index and `w` the weights
+__device__ __forceinline__ RescaleTap rescale_tap(int N, float c, float r, int stride, float w) {
   const int N2 = N / 2;
   const float rc = c / r;
   const int c1 = (int)floorf(rc), c2 = c1 + 1;
   const bool k1 = c1 > -N2 && c1 < N2, k2 = c2 > -N2 && c2 < N2;
   RescaleTap t;
-  t.w1 = k1 ? 1.f - fabsf((float)c1 - rc) : 0.f;
-  t.w2 = k2 ? 1.f - fabsf((float)c2 - rc) : 0.f;
-  t.i1 = k1 ? (c1 < 0 ? c1 + N : c1) * stride : -1;
-  t.i2 = k2 ? (c2 < 0 ? c2 + N : c2) * stride : -1;
+  t.w1 = k1 ? (1.f - fabsf((float)c1 - rc)) * w : 0.f;
+  t.w2 = k2 ? (1.f - fabsf((float)c2 - rc)) * w : 0.f;
+  t.i1 = k1 ? (c1 < 0 ? c1 + N : c1) * stride : 0;
+  t.i2 = k2 ? (c2 < 0 ? c2 + N : c2) * stride : 0;
   return t;
 }
 
 template <int N>
-__global__ void __launch_bounds__(kThreads, 6) pc_rescale_kernel(PcArgs a) {
+__global__ void __launch_bounds__(kThreads, 5) pc_rescale_kernel(PcArgs a) {
   using RT_ = RescaleTile<N>;
   constexpr int TC = RT_::TC, G = RT_::G, RB = RT_::RB, RT = RT_::RT, RQ = RT_::RQ;
   constexpr int N2 = N / 2;
   constexpr int TILES = (N / TC) * (N / RB);
   __shared__ RescaleTap yt[RQ][RB];
-  __shared__ float rq[RQ], wq[RQ];
+  __shared__ float rq[RQ];
   const int tc = threadIdx.x % TC, g = threadIdx.x / TC;
   for (int it = blockIdx.x; it < a.n_jobs * TILES; it += gridDim.x) {
     const int j = it / TILES, tile = it - j * TILES;
@@ -331,29 +333,21 @@ __global__ void __launch_bounds__(kThreads, 6) pc_rescale_kernel(PcArgs a) {
       __syncthreads();  // the previous tile or sample group is done with the tables
       for (int e = threadIdx.x; e < nq * RB; e += kThreads) {
         const int q = e / RB, r = r0 + e % RB;
-        yt[q][e % RB] = rescale_tap(N, (float)(r > N2 - 1 ? r - N : r), s.spec_r[q0 + q], N);
+        yt[q][e % RB] = rescale_tap(N, (float)(r > N2 - 1 ? r - N : r), s.spec_r[q0 + q], N,
+                                    s.spec_w[q0 + q]);
       }
-      if (threadIdx.x < nq) {
-        rq[threadIdx.x] = s.spec_r[q0 + threadIdx.x];
-        wq[threadIdx.x] = s.spec_w[q0 + threadIdx.x];
-      }
+      if (threadIdx.x < nq) rq[threadIdx.x] = s.spec_r[q0 + threadIdx.x];
       __syncthreads();
-#pragma unroll 2
       for (int q = 0; q < nq; ++q) {
-        const RescaleTap x = rescale_tap(N, xc, rq[q], 1);
-        const float sw = wq[q];
+        const RescaleTap x = rescale_tap(N, xc, rq[q], 1, 1.f);
 #pragma unroll
         for (int u = 0; u < RT; ++u) {
           const int lr = g + u * G;
           if (RB % G == 0 || lr < RB) {
             const RescaleTap y = yt[q][lr];
-            const float v11 = (x.i1 >= 0 && y.i1 >= 0) ? pp[y.i1 + x.i1] : 0.f;
-            const float v12 = (x.i1 >= 0 && y.i2 >= 0) ? pp[y.i2 + x.i1] : 0.f;
-            const float v21 = (x.i2 >= 0 && y.i1 >= 0) ? pp[y.i1 + x.i2] : 0.f;
-            const float v22 = (x.i2 >= 0 && y.i2 >= 0) ? pp[y.i2 + x.i2] : 0.f;
-            const float iv = v11 * x.w1 * y.w1 + v12 * x.w1 * y.w2 + v21 * x.w2 * y.w1 +
-                             v22 * x.w2 * y.w2;
-            cum[u] += iv * sw;
+            const float h1 = fmaf(pp[y.i1 + x.i2], x.w2, pp[y.i1 + x.i1] * x.w1);
+            const float h2 = fmaf(pp[y.i2 + x.i2], x.w2, pp[y.i2 + x.i1] * x.w1);
+            cum[u] = fmaf(y.w2, h2, fmaf(y.w1, h1, cum[u]));
           }
         }
       }
