@@ -431,7 +431,8 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       for (int p = 0; p < 2; ++p) {
         int per_sm = occ[p];
         if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, (int)opts->ctas_per_sm);
-        sg.grid[p] = std::max(1, std::min(count, sms * per_sm));
+        const int units = p == 0 ? count * col_split(N, E) : count;
+        sg.grid[p] = std::max(1, std::min(units, sms * per_sm));
       }
       for (int i = gstart[g]; i < gstart[g + 1]; ++i) {
         if (trials[i].n != N || !partial(trials[i])) continue;

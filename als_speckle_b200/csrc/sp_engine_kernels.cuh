@@ -61,9 +61,13 @@ struct Item {
 
 __host__ __device__ constexpr int clamp_e(int N, int E) { return E < N ? E : N; }
 
-// threads per line T = N / E, lines per item = min(256 / T, N)
+// threads per line T = N / E, lines per item = min(threads / T, N) for a
+// CTA of `threads` (kThreads = 256 unless a kernel says otherwise)
+__host__ __device__ constexpr int lines_per_item_t(int N, int E, int threads) {
+  return (threads / (N / clamp_e(N, E))) < N ? (threads / (N / clamp_e(N, E))) : N;
+}
 __host__ __device__ constexpr int lines_per_item(int N, int E) {
-  return (kThreads / (N / clamp_e(N, E))) < N ? (kThreads / (N / clamp_e(N, E))) : N;
+  return lines_per_item_t(N, E, kThreads);
 }
 
 // Algorithm of 1-based iteration i: order_list[(i-1) % period] (phasing.py:260-267)
@@ -221,10 +225,12 @@ __host__ __device__ constexpr int next_congruent(int x, int r, int m) {
 // thread has just consumed.  With SP = 16/C (mod 16) for C <= 8 and SP odd
 // for C >= 16, every half-warp of those accesses touches 16 distinct 8-byte
 // bank pairs; MP staggers the modulus strips of columns that share a warp.
-template <int N, int E>
+// TH is the CTA's thread count and NB its number of G buffers (two for the
+// pipelined column pass, one for the single-buffered one).
+template <int N, int E, int TH = kThreads, int NB = 2>
 struct ColSmem {
   static constexpr int T = N / E;
-  static constexpr int C = lines_per_item(N, E);
+  static constexpr int C = lines_per_item_t(N, E, TH);
   static constexpr int SH = pad_shift(E);
   static constexpr int SP = C >= 16 ? next_congruent(padk(N, SH), 1, 2)
                                     : next_congruent(padk(N, SH), 16 / C, 16);
@@ -233,7 +239,7 @@ struct ColSmem {
   static constexpr int RL = N / NSL;             // last stage radix
   static constexpr int BF = C * NSL;             // last-stage butterflies per item
   static constexpr int kB = C * SP;              // float2 entries per G buffer
-  static constexpr int kTw = 2 * kB;             // offset of the twiddle tables
+  static constexpr int kTw = NB * kB;            // offset of the twiddle tables
   static constexpr int kMod = kTw + tw_stage_total(N, E);  // offset of the modulus strips
   static constexpr int kTotal = kMod + (C * MP + 1) / 2;
   // line groups for the modulus copy: GT threads own CG columns
@@ -559,18 +565,18 @@ __device__ __forceinline__ bool col_projects(const Slot& s, int tick) {
 // This thread's last-stage butterflies of a column item: butterfly u is row
 // j(u) of column c, and pa(u, r) the strip offset of its row j(u) + r*NSL in
 // a G buffer.
-template <int N, int E>
+template <int N, int E, int TH = kThreads>
 struct ColButterflies {
-  using CS = ColSmem<N, E>;
+  using CS = ColSmem<N, E, TH>;
   static constexpr int C = CS::C, SH = CS::SH, P = 1 << SH;
-  static constexpr int U = (CS::BF + kThreads - 1) / kThreads;
-  static constexpr int JS = kThreads / C;  // row step between a thread's butterflies
+  static constexpr int U = (CS::BF + TH - 1) / TH;
+  static constexpr int JS = TH / C;  // row step between a thread's butterflies
   static constexpr bool LIN = (JS % P) == 0 && (CS::NSL % P) == 0;
   int c, j0, pj0;
   __device__ __forceinline__ ColButterflies()
       : c(threadIdx.x % C), j0(threadIdx.x / C), pj0(c * CS::SP + padk(j0, SH)) {}
   __device__ __forceinline__ bool valid(int u) const {
-    return CS::BF % kThreads == 0 || j0 + u * JS < CS::NSL;
+    return CS::BF % TH == 0 || j0 + u * JS < CS::NSL;
   }
   __device__ __forceinline__ int j(int u) const { return j0 + u * JS; }
   __device__ __forceinline__ int pa(int u, int r) const {
@@ -580,10 +586,10 @@ struct ColButterflies {
 };
 
 // Request the tile of a column item from the plane `plane`, in the row mapping.
-template <int N, int E>
+template <int N, int E, int TH = kThreads>
 __device__ __forceinline__ void copy_col_plane(const float2* plane, int block, float2* gbuf) {
-  using CS = ColSmem<N, E>;
-  using BF = ColButterflies<N, E>;
+  using CS = ColSmem<N, E, TH>;
+  using BF = ColButterflies<N, E, TH>;
   const BF bf;
   const float2* g = plane + block * CS::C + bf.c;
 #pragma unroll
@@ -597,9 +603,9 @@ __device__ __forceinline__ void copy_col_plane(const float2* plane, int block, f
 }
 
 // Request the G tile of a column item when it projects.
-template <int N, int E>
+template <int N, int E, int TH = kThreads>
 __device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, float2* gbuf) {
-  if (col_projects(s, tick)) copy_col_plane<N, E>(s.g, block, gbuf);
+  if (col_projects(s, tick)) copy_col_plane<N, E, TH>(s.g, block, gbuf);
 }
 
 // The last stage of the inverse column transforms of an item whose earlier
@@ -610,11 +616,11 @@ __device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, f
 // row pass.  All inputs are read first; `then()` runs before the
 // arithmetic (the caller's next copies into gbuf go there: each overwrites
 // only entries this thread has already read).
-template <int N, int E, class Then>
+template <int N, int E, int TH = kThreads, class Then>
 __device__ __forceinline__ void col_last_stage(float2* g, int block, const float2* gbuf,
                                                const float2* __restrict__ tw, Then&& then) {
-  using CS = ColSmem<N, E>;
-  using BF = ColButterflies<N, E>;
+  using CS = ColSmem<N, E, TH>;
+  using BF = ColButterflies<N, E, TH>;
   constexpr int R = CS::RL, NS = CS::NSL;
   const float2* __restrict__ tws = tw + tw_stage_offset(N, E, NS);
   const BF bf;
@@ -643,9 +649,9 @@ __device__ __forceinline__ void col_last_stage(float2* g, int block, const float
 
 // Each column's threads request their columns' modulus: rows of the
 // transposed modulus, 16 bytes per cp.async, into the columns' strips.
-template <int N, int E>
+template <int N, int E, int TH = kThreads>
 __device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick, float* mod) {
-  using CS = ColSmem<N, E>;
+  using CS = ColSmem<N, E, TH>;
   if (!col_live(s, tick)) return;
   const int g = threadIdx.x / CS::GT;
   const int gtid = threadIdx.x - g * CS::GT;
@@ -672,15 +678,15 @@ __device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick,
 // to its last stage.  Returns the plane that col_last_stage must complete
 // (for DM the first plane is finished here and the second plane's tile
 // brought into the strips, which its transforms need).
-template <int N, int E>
+template <int N, int E, int TH = kThreads>
 __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, float2* gbuf,
                                             const float* mod, const float2* __restrict__ tw) {
-  using CS = ColSmem<N, E>;
+  using CS = ColSmem<N, E, TH>;
   constexpr int T = CS::T;
   constexpr int C = CS::C;
   constexpr int SH = CS::SH, P = 1 << SH;
   constexpr float inv = 1.0f / ((float)N * (float)N);
-  constexpr bool kFull = (C * T == kThreads);
+  constexpr bool kFull = (C * T == TH);
   using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
   const int tid = threadIdx.x;
   const int lcol = tid / T;
@@ -751,8 +757,8 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
       // finish G and bring in the G2 tile through the same strips (each
       // thread's copies overwrite only entries it has already read)
       __syncthreads();  // every column's last-stage inputs are in the strips
-      col_last_stage<N, E>(s.g, block, gbuf, tw, [&] {
-        copy_col_plane<N, E>(s.g2, block, gbuf);
+      col_last_stage<N, E, TH>(s.g, block, gbuf, tw, [&] {
+        copy_col_plane<N, E, TH>(s.g2, block, gbuf);
         asm volatile("cp.async.commit_group;" ::: "memory");
       });
       cp_async_wait_all();

@@ -188,30 +188,120 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
   cp_async_wait_all();
 }
 
+// Single-buffered column pass: CTAs of kColSbThreads threads, each walking
+// half items (C/2 columns; sub-item j is half j & 1 of item j >> 1), with one
+// G buffer, so three CTAs (12 warps) fit an SM where the pipelined form fits
+// one of 8 warps.  A CTA does not overlap its next tile's copy with its own
+// work; the other CTAs on the SM cover it.  Per half item: wait for the tile,
+// barrier, forward transform, projection and inverse transform up to its
+// last stage (col_item), barrier, then the last stage in the row mapping
+// straight to global memory, requesting the next half's modulus and tile
+// into the same buffer as its inputs are consumed (each thread overwrites
+// only entries it has read).  Used where it measures faster (512^2 at E = 32;
+// at 1024^2 and above its narrower tiles lose more than the extra warps gain).
+constexpr int kColSbThreads = 128;
+__host__ __device__ constexpr bool col_single_buffered(int N, int E) { return N == 512 && E == 32; }
+// column-pass work units per item
+__host__ __device__ constexpr int col_split(int N, int E) {
+  return col_single_buffered(N, E) ? lines_per_item(N, E) / lines_per_item_t(N, E, kColSbThreads) : 1;
+}
+
 template <int N, int E>
-constexpr size_t col_smem_bytes() { return (size_t)ColSmem<N, E>::kTotal * sizeof(float2); }
+__global__ void __launch_bounds__(kColSbThreads, 3) col_pass_sb_kernel(PassArgs a) {
+  constexpr int TH = kColSbThreads;
+  constexpr int SPLIT = col_split(N, E);
+  using CS = ColSmem<N, E, TH, 1>;
+  static_assert(SPLIT * CS::C == lines_per_item(N, E), "an item is SPLIT whole sub-items");
+  extern __shared__ float2 smem[];
+  __shared__ __align__(16) Slot sl[3];
+  const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
+  const float2* tw = stage_twiddles<N, E>(smem + CS::kTw, a.tw);  // block barrier
+  float* mod = reinterpret_cast<float*>(smem + CS::kMod);
+  const int n_sub = SPLIT * a.n_items;
+  int it = blockIdx.x;
+  if (it >= n_sub) return;  // the whole block leaves together
+  const int G = gridDim.x;
+  auto sub_at = [&](int j) -> Item {
+    if (j >= n_sub) return Item{-1, 0};
+    Item i = item_at(a, j / SPLIT);
+    i.block = SPLIT * i.block + j % SPLIT;
+    return i;
+  };
+  // sub-items k, k+1, k+2 held in registers; sub-item k+3 is read during k
+  Item i0 = sub_at(it), i1 = sub_at(it + G), i2 = sub_at(it + 2 * G);
+  load_slot(&sl[0], &a.slots[i0.slot]);
+  if (i1.slot >= 0) load_slot(&sl[1], &a.slots[i1.slot]);
+  __syncthreads();
+  copy_col_mod<N, E, TH>(sl[0], i0.block, tick, mod);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  copy_col_g<N, E, TH>(sl[0], i0.block, tick, smem);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int k = 0; it < n_sub; it += G, ++k) {
+    const Item i3 = sub_at(it + 3 * G);
+    cp_async_wait_all();  // this sub-item's modulus and tile, sub-item k+1's descriptor
+    __syncthreads();      // ... visible to all; the previous sub-item is finished
+    const Slot& s = sl[k % 3];
+    float2* pend = nullptr;
+    if (col_live(s, tick)) pend = col_item<N, E, TH>(s, tick - s.start_tick, i0.block, smem, mod, tw);
+    __syncthreads();  // last-stage inputs in the strips; the modulus strips consumed
+    auto copies = [&]() {
+      if (i1.slot >= 0) copy_col_mod<N, E, TH>(sl[(k + 1) % 3], i1.block, tick, mod);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      if (i1.slot >= 0) copy_col_g<N, E, TH>(sl[(k + 1) % 3], i1.block, tick, smem);
+      if (i2.slot >= 0) copy_slot(&sl[(k + 2) % 3], &a.slots[i2.slot]);  // sub-item k-1's entry
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (pend)
+      col_last_stage<N, E, TH>(pend, i0.block, smem, tw, copies);
+    else
+      copies();
+    i0 = i1;
+    i1 = i2;
+    i2 = i3;
+  }
+  cp_async_wait_all();
+}
+
+template <int N, int E>
+constexpr size_t col_smem_bytes() {
+  if constexpr (col_single_buffered(N, E))
+    return (size_t)ColSmem<N, E, kColSbThreads, 1>::kTotal * sizeof(float2);
+  else
+    return (size_t)ColSmem<N, E>::kTotal * sizeof(float2);
+}
 template <int N, int E>
 constexpr size_t row_smem_bytes() { return (size_t)RowSmem<N, E>::kTotal * sizeof(float2); }
 
 template <int N, int E>
 cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& a) {
-  if (which == 0)
-    col_pass_kernel<N, E><<<grid, kThreads, col_smem_bytes<N, E>(), st>>>(a);
-  else
+  if (which == 0) {
+    if constexpr (col_single_buffered(N, E))
+      col_pass_sb_kernel<N, E><<<grid, kColSbThreads, col_smem_bytes<N, E>(), st>>>(a);
+    else
+      col_pass_kernel<N, E><<<grid, kThreads, col_smem_bytes<N, E>(), st>>>(a);
+  } else
     row_pass_kernel<N, E><<<grid, kThreads, row_smem_bytes<N, E>(), st>>>(a);
   return cudaGetLastError();
 }
 
 // occupancy[0] = resident column-pass CTAs per SM, occupancy[1] = row-pass
+// (the column pass's CTAs each take 1 / col_split(N, E) of an item)
 template <int N, int E>
 cudaError_t pass_setup_t(int* occupancy) {
   const int sc = (int)col_smem_bytes<N, E>(), sr = (int)row_smem_bytes<N, E>();
   cudaError_t e;
-  e = cudaFuncSetAttribute(col_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc);
+  if constexpr (col_single_buffered(N, E)) {
+    e = cudaFuncSetAttribute(col_pass_sb_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[0], col_pass_sb_kernel<N, E>,
+                                                      kColSbThreads, sc);
+  } else {
+    e = cudaFuncSetAttribute(col_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[0], col_pass_kernel<N, E>, kThreads, sc);
+  }
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(row_pass_kernel<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
-  if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[0], col_pass_kernel<N, E>, kThreads, sc);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy[1], row_pass_kernel<N, E>, kThreads, sr);
 }

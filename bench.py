@@ -330,7 +330,7 @@ def run_ours(args):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": "sp::col_pass_kernel<512,E> + sp::row_pass_kernel<512,E> "
+                     "kernel": "sp::col_pass_sb_kernel<512,32> + sp::row_pass_kernel<512,32> "
                                "(one iteration tick of %d trials, 24 B/px)" % group,
                      "traffic": traffic_per_tick(group)},
         "plain_gpu": plain,
