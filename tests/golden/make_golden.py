@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 if len(sys.argv) > 1:
     os.environ["SPECKLE_REF_ROOT"] = sys.argv[1]
+import golden_inputs as inputs  # noqa: E402
 import refshim  # noqa: E402
 
 ref = refshim.load_reference()
@@ -31,19 +32,7 @@ def _quiet(fn, *a, **k):
 
 
 def _inputs(N, seed):
-    rng = np.random.default_rng(seed)
-    # a smooth object in a centred box, its modulus, and a square support
-    B = max(2, N // 4)
-    obj = np.zeros((N, N), np.complex128)
-    c = N // 2
-    box = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.7, 0.7, (B, B)))
-    obj[c - B // 2:c - B // 2 + B, c - B // 2:c - B // 2 + B] = box
-    modulus = np.abs(np.fft.fft2(obj)).astype(np.float32)
-    support = np.zeros((N, N), np.float32)
-    S = min(N, B + max(2, N // 8))
-    support[c - S // 2:c - S // 2 + S, c - S // 2:c - S // 2 + S] = 1
-    psi = (rng.random((N, N)) + 1j * rng.random((N, N))).astype(np.complex64) * support
-    return psi.astype(np.complex64), modulus, support
+    return inputs.projection_inputs(N, seed)
 
 
 def projections():
@@ -66,6 +55,36 @@ def projections():
             out["N%d_%s_savebuffer" % (N, alg)] = np.asarray(r.savebuffer)
             out["N%d_%s_box" % (N, alg)] = np.array([r.r0, r.rows, r.c0, r.cols])
     np.savez_compressed(os.path.join(HERE, "projections.npz"), **out)
+
+
+def projections_large(samples=4096):
+    """One reference iteration of each algorithm at 256^2 and 512^2.  The
+    inputs are rebuilt by the tests from ``inputs.projection_inputs``; the
+    outputs are stored at ``samples`` fixed pixels (the same for every
+    algorithm) plus FP64 whole-plane sums, which keeps the fixture small."""
+    out = {}
+    for N in (256, 512):
+        seed = 100 + N
+        psi, modulus, support = _inputs(N, seed)
+        out["N%d_seed" % N] = np.int64(seed)
+        out["N%d_input_sums" % N] = inputs.input_sums(psi, modulus, support)
+        idx = np.random.default_rng(7 + N).choice(N * N, samples, replace=False)
+        # half of the samples inside the support, where the update keeps the projection
+        inside = np.flatnonzero(support.ravel() > 0)
+        idx[: samples // 2] = np.random.default_rng(8 + N).choice(inside, samples // 2, replace=False)
+        out["N%d_idx" % N] = idx.astype(np.int64)
+        for alg in ("hio", "er", "raar", "sf", "dm"):
+            beta = 0.9 if alg != "raar" else 0.87
+            r = _quiet(ref.phasing.phasing, force_cpu=True, force_np_fft=True)
+            _quiet(r.load, modulus=modulus, support=support, numtrials=1)
+            r.psi_in = psi.copy()
+            _quiet(r.iterate, 1, order=((alg, 1),), beta=beta)
+            res = np.asarray(r.psi_in).astype(np.complex128)
+            out["N%d_%s_beta" % (N, alg)] = np.float64(beta)
+            out["N%d_%s_samples" % (N, alg)] = res.ravel()[idx].astype(np.complex64)
+            out["N%d_%s_sums" % (N, alg)] = np.array(
+                [np.sum(np.abs(res) ** 2), np.sum(res).real, np.sum(res).imag])
+    np.savez_compressed(os.path.join(HERE, "projections_large.npz"), **out)
 
 
 def trajectories():
@@ -252,6 +271,7 @@ def coherence_opt():
 
 if __name__ == "__main__":
     projections()
+    projections_large()
     trajectories()
     seeds()
     helpers()

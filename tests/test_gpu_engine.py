@@ -67,6 +67,31 @@ def test_single_projection_vs_reference_golden(engine, N, alg):
     assert rel(psi.cpu().numpy(), g["N%d_%s_psi_in" % (N, alg)]) < 1e-5
 
 
+@pytest.mark.parametrize("N", [256, 512])
+@pytest.mark.parametrize("alg", ["hio", "er", "raar", "sf", "dm"])
+def test_single_projection_vs_reference_golden_large(engine, N, alg):
+    """One iteration at 256^2 and 512^2 against the reference's own numpy
+    path: its output at 4096 fixed pixels (half inside the support) and its
+    FP64 whole-plane sums, on inputs rebuilt from the fixture's seed."""
+    import sys
+    sys.path.insert(0, G)
+    import golden_inputs as inputs
+    g = np.load(os.path.join(G, "projections_large.npz"))
+    psi0, M, S = inputs.projection_inputs(N, int(g["N%d_seed" % N]))
+    np.testing.assert_allclose(inputs.input_sums(psi0, M, S), g["N%d_input_sums" % N], rtol=1e-12)
+    psi = dev(psi0)
+    beta = float(g["N%d_%s_beta" % (N, alg)])
+    engine.solve([_spec(psi, dev(M), dev(S), 1, ((alg, 1),), beta, quirks="cpu")])
+    got = psi.cpu().numpy()
+    assert rel(got.ravel()[g["N%d_idx" % N]], g["N%d_%s_samples" % (N, alg)]) < 1e-5
+    r = got.astype(np.complex128)
+    sums = np.array([np.sum(np.abs(r) ** 2), np.sum(r).real, np.sum(r).imag])
+    want = g["N%d_%s_sums" % (N, alg)]
+    assert abs(sums[0] - want[0]) / want[0] < 1e-5
+    scale = np.sqrt(want[0] * r.size)  # bound on |sum| by Cauchy-Schwarz
+    assert np.all(np.abs(sums[1:] - want[1:]) / scale < 1e-5)
+
+
 @pytest.mark.parametrize("E", [8, 16, 32])
 @pytest.mark.parametrize("N", [128, 256, 512, 1024, 2048])
 @pytest.mark.parametrize("alg", ["hio", "er", "raar", "sf", "dm"])
