@@ -330,8 +330,10 @@ def run_ours(args):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": "sp::col_pass_sb_kernel<512,32> + sp::row_pass_kernel<512,32> "
-                               "(one iteration tick of %d trials, 24 B/px)" % group,
+                     "kernel": "%s + sp::row_pass_kernel<512,%d> (one iteration tick of %d trials, "
+                               "24 B/px)" % ("sp::col_pass_sb_kernel<512,32>" if tune["E"] >= 32 else
+                                             "sp::col_pass_kernel<512,%d>" % tune["E"], min(tune["E"], 32),
+                                             group),
                      "traffic": traffic_per_tick(group)},
         "plain_gpu": plain,
         "single_trial_engine": single,
