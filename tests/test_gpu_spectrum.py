@@ -72,6 +72,24 @@ def test_spectrum_projection_vs_fp64_oracle(engine, N, alg, with_ipsf):
     assert rel(plain, want) > 1e-3  # the spectrum changes the result
 
 
+# 21 samples (more than the 16 the rescale kernel tabulates per pass), and
+# factors from 0.4 to 2.5: taps far outside (-N/2, N/2) (weight 0, read at
+# their coordinate modulo N) and strongly magnified ones.
+SPEC_WIDE = np.array([np.concatenate([np.linspace(0.4, 0.9, 10), [1.0], np.linspace(1.1, 2.5, 10)]),
+                      np.concatenate([np.linspace(0.1, 0.9, 10), [1.0], np.linspace(0.9, 0.1, 10)])])
+
+
+@pytest.mark.parametrize("N", [256, 2048])
+def test_spectrum_many_wide_samples_vs_fp64_oracle(engine, N):
+    from als_speckle_b200.engine import TrialSpec
+    M, S, psi0 = _case(N, seed=3)
+    want, _ = O.iteration(psi0, M, S, "hio", 0.9, mode="f64", spectrum=SPEC_WIDE)
+    psi = dev(psi0)
+    engine.solve([TrialSpec(psi=psi, modulus=dev(M), support=dev(S), iterations=1,
+                            order=(("hio", 1),), beta=0.9, spectrum=_spectrum_dev(SPEC_WIDE))])
+    assert rel(psi.cpu().numpy(), want) < 1e-5
+
+
 def test_spectrum_batch_equals_alone(engine):
     """Spectrum, ipsf and coherent trials together give the same bits as alone."""
     from als_speckle_b200.engine import TrialSpec
