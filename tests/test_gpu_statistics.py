@@ -1,12 +1,17 @@
 """Statistical parity over 32 seeds.
 
 Projection iterations are chaotic, so long runs are compared by distribution:
-32 seeded random-phase starts (identical starts on both sides) iterated
-100 HIO (beta 0.9) + 20 ER at N = 128 on the GPU and in the FP64 oracle.
-The final R-factors must agree in mean to 1% and pass a two-sample
-Kolmogorov-Smirnov test, and the annular PRTFs of the two sets of
-reconstructions must agree to 0.05 per annulus.
+32 seeded random-phase starts (identical starts on both sides) iterated on
+the GPU and in the FP64 oracle — 100 HIO (beta 0.9) + 20 ER at N = 128, and
+the plain 256^2 configuration (20 ellipses, 1e5 photons, 80^2 support,
+200 HIO + 20 ER).  The final R-factors must agree in mean to 1% and pass a
+two-sample Kolmogorov-Smirnov test, and the annular PRTFs of the two sets of
+reconstructions must agree to 0.05 per annulus.  The oracle's trials run in
+a spawned process pool (the test process has already initialised CUDA).
 """
+import multiprocessing as mp
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -17,6 +22,21 @@ pytestmark = pytest.mark.gpu
 
 N, SEEDS, ORDER, ITERS, BETA = 128, 32, (("hio", 100), ("er", 20)), 120, 0.9
 
+CASES = {
+    "small128": dict(N=128, pattern=dict(n_ellipses=10, box=32, peak=1e5, seed=3, support_edge=40),
+                     order=(("hio", 100), ("er", 20))),
+    "plain256": dict(N=256, pattern=dict(n_ellipses=20, box=64, peak=1e5, seed=0, support_edge=80),
+                     order=(("hio", 200), ("er", 20))),
+}
+
+
+def _oracle_trial(args):
+    """One FP64 oracle trial from the seeded random-phase start (pool worker)."""
+    M, S, k, order, iters, box = args
+    psi = O.seed_random_phase(M, S, 77, k)
+    psi, e = O.iterate(psi, M, S, iters, order=order, beta=BETA, mode="f64", errors=True)
+    return e[-1, 1], O.crop(psi, box[0], box[1], box[2], box[3])
+
 
 def _annular(p):
     n = p.shape[0]
@@ -26,43 +46,45 @@ def _annular(p):
     return np.bincount(r[keep], weights=p[keep]) / np.maximum(np.bincount(r[keep]), 1)
 
 
-def test_final_r_factor_and_prtf_distributions_match_oracle():
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_final_r_factor_and_prtf_distributions_match_oracle(case):
     from scipy.stats import ks_2samp
     from als_speckle_b200 import synth
     from als_speckle_b200.engine import Engine, TrialSpec
     from als_speckle_b200.masking import bounding_box
-    _, M, S = synth.pattern(N, n_ellipses=10, box=32, peak=1e5, seed=3, support_edge=40)
+    c = CASES[case]
+    n, order = c["N"], c["order"]
+    iters = sum(k for _, k in order)
+    _, M, S = synth.pattern(n, **c["pattern"])
     bb = bounding_box(S, pad=10)
     box = (int(bb[0]), int(bb[2]), int(bb[1] - bb[0]), int(bb[3] - bb[2]))
     m = M.astype(np.float64)
 
     # GPU
     Md, Sd = torch.from_numpy(M).cuda(), torch.from_numpy(S).cuda()
-    psis = torch.zeros((SEEDS, N, N), dtype=torch.complex64, device="cuda")
+    psis = torch.zeros((SEEDS, n, n), dtype=torch.complex64, device="cuda")
     saves = torch.zeros((SEEDS, box[2], box[3]), dtype=torch.complex64, device="cuda")
-    errs = torch.zeros((SEEDS, ITERS, 2), dtype=torch.float64, device="cuda")
+    errs = torch.zeros((SEEDS, iters, 2), dtype=torch.float64, device="cuda")
     eng = Engine(use_graph=False)
-    eng.solve([TrialSpec(psi=psis[k], modulus=Md, support=Sd, iterations=ITERS, order=ORDER,
+    eng.solve([TrialSpec(psi=psis[k], modulus=Md, support=Sd, iterations=iters, order=order,
                          beta=BETA, random_phase=True, seed=77, trial=k, box=box, save=saves[k],
                          errors=errs[k]) for k in range(SEEDS)])
     torch.cuda.synchronize()
     r_gpu = errs[:, -1, 1].cpu().numpy() / np.sum(m)
 
-    # FP64 oracle from the same starts
-    r_ref, crops = [], []
-    for k in range(SEEDS):
-        psi = O.seed_random_phase(M, S, 77, k)
-        psi, e = O.iterate(psi, M, S, ITERS, order=ORDER, beta=BETA, mode="f64", errors=True)
-        r_ref.append(e[-1, 1])
-        crops.append(O.crop(psi, box[0], box[1], box[2], box[3]))
-    r_ref = np.array(r_ref)
+    # FP64 oracle from the same starts, one trial per worker
+    workers = max(1, min(16, len(os.sched_getaffinity(0))))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        res = pool.map(_oracle_trial, [(M, S, k, order, iters, box) for k in range(SEEDS)])
+    r_ref = np.array([r for r, _ in res])
+    crops = [cr for _, cr in res]
 
     assert abs(r_gpu.mean() - r_ref.mean()) / r_ref.mean() < 0.01
     assert ks_2samp(r_gpu, r_ref).pvalue > 0.01
 
     from als_speckle_b200.phasing import align_global_phase, prtf
-    p_gpu = prtf(align_global_phase(saves), N=N).cpu().numpy()
-    p_ref = O.prtf(O.align_global_phase(np.array(crops)), N=N)
+    p_gpu = prtf(align_global_phase(saves), N=n).cpu().numpy()
+    p_ref = O.prtf(O.align_global_phase(np.array(crops)), N=n)
     assert np.max(np.abs(_annular(p_gpu) - _annular(p_ref))) < 0.05
     eng.close()
 
