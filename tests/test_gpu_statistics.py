@@ -4,7 +4,8 @@ Projection iterations are chaotic, so long runs are compared by distribution:
 32 seeded random-phase starts (identical starts on both sides) iterated on
 the GPU and in the FP64 oracle — 100 HIO (beta 0.9) + 20 ER at N = 128, and
 the plain 256^2 configuration (20 ellipses, 1e5 photons, 80^2 support,
-200 HIO + 20 ER).  The final R-factors must agree in mean to 1% and pass a
+200 HIO + 20 ER), and the benchmark's 512^2 configuration (40 ellipses,
+1e6 photons, 160^2 support, 500 HIO + 50 ER).  The final R-factors must agree in mean to 1% and pass a
 two-sample Kolmogorov-Smirnov test, and the annular PRTFs of the two sets of
 reconstructions must agree to 0.05 per annulus.  The oracle's trials run in
 a spawned process pool (the test process has already initialised CUDA).
@@ -27,6 +28,8 @@ CASES = {
                      order=(("hio", 100), ("er", 20))),
     "plain256": dict(N=256, pattern=dict(n_ellipses=20, box=64, peak=1e5, seed=0, support_edge=80),
                      order=(("hio", 200), ("er", 20))),
+    "hio512": dict(N=512, pattern=dict(n_ellipses=40, box=128, peak=1e6, seed=0, support_edge=160),
+                   order=(("hio", 500), ("er", 50))),
 }
 
 
