@@ -42,6 +42,16 @@ def load(path=CACHE):
         return {}
 
 
+def tuned_e_per_n(path=CACHE, device_name=None):
+    """{N: E} for every size tuned on this device (empty when none was)."""
+    entries = load(path).get(device_name or _device_key(), {})
+    out = {}
+    for n, entry in entries.items():
+        if isinstance(entry, dict) and "E" in entry:
+            out[int(n)] = int(entry["E"])
+    return out
+
+
 def load_or_default(N, path=CACHE):
     entry = load(path).get(_device_key(), {}).get(str(N))
     out = dict(DEFAULTS)

@@ -136,7 +136,11 @@ class Engine:
     ``l2_group_bytes`` groups trials so each group's planes stay in L2 while it
     iterates; ``use_graph`` captures each group's launches in a CUDA graph
     (cached per workspace and shape); ``e_per_n`` maps N to the per-thread
-    radix E (16 or 32) picked by ``autotune``.
+    radix E (16 or 32).  Left as None it is the autotuner's table for this
+    device (``autotune.json``), so every caller gets the tuned E per size;
+    ``{}`` leaves every size to the library's default (E = 32).  The choice
+    depends only on N, never on how many trials a call carries, so a trial's
+    result is the same alone and batched with others.
     """
 
     def __init__(self, device=None, l2_group_bytes=0, use_graph=True, e_per_n=None,
@@ -144,7 +148,13 @@ class Engine:
         self.device = torch.device(device if device is not None else "cuda")
         self.l2_group_bytes = int(l2_group_bytes)
         self.use_graph = bool(use_graph)
-        self.e_per_n = dict(e_per_n or {})
+        if e_per_n is None:
+            e_per_n = {}
+            if torch.cuda.is_available():
+                from . import autotune
+                with torch.cuda.device(self.device):
+                    e_per_n = autotune.tuned_e_per_n()
+        self.e_per_n = dict(e_per_n)
         self.ctas_per_sm = int(ctas_per_sm)
         self._ws = None
 

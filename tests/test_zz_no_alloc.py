@@ -58,9 +58,10 @@ def test_static_entry_matches_workspace_entry_twice():
     from als_speckle_b200.engine import Engine, _to_struct
     inp = _trials()
 
-    # reference result: the existing entry point with a torch-allocated workspace
+    # reference result: the existing entry point with a torch-allocated workspace,
+    # with the library's default E per size, as the static call below uses
     psis, saves, errs = _buffers(inp)
-    eng = Engine(use_graph=False)
+    eng = Engine(use_graph=False, e_per_n={})
     eng.solve(_specs(inp, psis, saves, errs))
     torch.cuda.synchronize()
 
