@@ -75,3 +75,22 @@ def test_synthetic_generator_properties():
     assert np.all(np.abs(obj[np.abs(obj) > 0]) <= 1.0 + 1e-12)
     o2, m2, s2 = synth.pattern(256, n_ellipses=20, box=64, peak=1e5, seed=1, support_edge=80)
     assert np.array_equal(m2, modulus)
+
+
+def test_tuned_e_table(tmp_path):
+    """The engine's default E per size comes from the tuning file's entry for
+    the device; sizes without an E and other devices are ignored."""
+    import json
+    from als_speckle_b200 import autotune
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({
+        "Dev A": {"256": {"E": 16, "rate": 1.0}, "512": {"E": 32}, "1024": {"rate": 2.0}},
+        "Dev B": {"256": {"E": 32}},
+    }))
+    assert autotune.tuned_e_per_n(str(path), "Dev A") == {256: 16, 512: 32}
+    assert autotune.tuned_e_per_n(str(path), "Dev C") == {}
+    assert autotune.tuned_e_per_n(str(tmp_path / "missing.json"), "Dev A") == {}
+    # the committed table names E for every size the benchmarks use on B200
+    table = autotune.tuned_e_per_n(device_name="NVIDIA B200")
+    assert set(table) >= {256, 512, 1024, 2048}
+    assert all(e in (8, 16, 32) for e in table.values())
