@@ -31,3 +31,34 @@ def input_sums(psi, modulus, support):
     """FP64 fingerprints of the inputs: sum |psi|^2, sum M, sum S."""
     return np.array([np.sum(np.abs(psi.astype(np.complex128)) ** 2),
                      np.sum(modulus.astype(np.float64)), np.sum(support.astype(np.float64))])
+
+
+def prtf_estimates(N, frames, seed):
+    """``frames`` N x N reconstructions of one object (a random complex box
+    of edge N/4 at the centre) with independent noise and phase offsets, as a
+    set of aligned trials looks: the PRTF input of the unwrap fixtures."""
+    rng = np.random.default_rng(seed)
+    B = max(2, N // 4)
+    c = N // 2
+    obj = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.6, 0.6, (B, B)))
+    out = np.zeros((frames, N, N), np.complex64)
+    for f in range(frames):
+        noisy = obj + 0.15 * (rng.standard_normal((B, B)) + 1j * rng.standard_normal((B, B)))
+        out[f, c - B // 2:c - B // 2 + B, c - B // 2:c - B // 2 + B] = noisy * np.exp(1j * rng.uniform(-0.2, 0.2))
+    return out
+
+
+def smooth_map(N, seed):
+    """A smooth float32 N x N map (a few Gaussian bumps and a radial falloff
+    plus mild noise) with structure at every radius: the input of the
+    large-N unwrap fixture."""
+    rng = np.random.default_rng(seed)
+    y, x = np.indices((N, N)).astype(np.float64)
+    r = np.hypot(y - N // 2, x - N // 2)
+    m = np.exp(-r / (0.35 * N))
+    for _ in range(6):
+        cy, cx = rng.uniform(0.1 * N, 0.9 * N, 2)
+        s = rng.uniform(0.02, 0.08) * N
+        m += rng.uniform(0.2, 0.8) * np.exp(-((y - cy) ** 2 + (x - cx) ** 2) / (2 * s * s))
+    m += 0.02 * rng.random((N, N))
+    return m.astype(np.float32)

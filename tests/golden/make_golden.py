@@ -5,7 +5,7 @@ loaded unmodified through ``refshim``) on fixed, seeded inputs and stores
 inputs and outputs as ``.npz`` files.  Run it from the repository root in a
 container that has the reference checkout:
 
-    python tests/golden/make_golden.py [reference_root]
+    python tests/golden/make_golden.py <reference_root> [fixture ...]
 
 The tests read only the ``.npz`` files; they never need the reference.
 """
@@ -269,15 +269,46 @@ def coherence_opt():
     np.savez_compressed(os.path.join(HERE, "coherence_opt.npz"), **out)
 
 
+def unwraps():
+    """The polar-unwrap outputs (``prtfq``, ``rftfq``): ``prtf(prtfq=True)``
+    on seeded trial sets at N = 32 and 64, ``rftf(rftfq=True)`` on the
+    quality fixture's inputs, and ``wrapping.unwrap`` of a smooth 512 x 512
+    map (row means, a sample of the unwrapped pixels)."""
+    out = {}
+    for N, frames in ((32, 6), (64, 8)):
+        est = inputs.prtf_estimates(N, frames, 40 + N)
+        out["prtf%d_in" % N] = est
+        arr, q = _quiet(ref.phasing.prtf, est, prtfq=True)
+        out["prtf%d_array" % N], out["prtf%d_q" % N] = arr, q
+    for N in (32, 64):
+        rng = np.random.default_rng(500 + N)   # the inputs of quality()
+        B = N // 4
+        obj = np.zeros((N, N), np.complex128)
+        obj[:B, :B] = rng.random((B, B)) * np.exp(1j * rng.uniform(-0.5, 0.5, (B, B)))
+        goal = (np.abs(np.fft.fft2(obj)) + 0.05).astype(np.float32)
+        est = (obj[:B, :B] + 0.05 * rng.standard_normal((B, B))).astype(np.complex64)
+        for name, kw in (("plain", {}), ("scale", {"scale": True})):
+            arr, q = ref.phasing.rftf(est, goal, rftfq=True, **kw)
+            out["rftf%d_%s_q" % (N, name)] = q
+    N = 512
+    m = inputs.smooth_map(N, 77)
+    out["map512_sums"] = np.array([np.sum(m.astype(np.float64)), np.sum(m.astype(np.float64) ** 2)])
+    uw = ref.wrapping.unwrap(m, (0, N // 2, (N // 2, N // 2)))
+    out["map512_mean"] = np.average(uw, axis=1)
+    idx = np.random.default_rng(3).choice(uw.size, 4096, replace=False)
+    out["map512_idx"] = idx.astype(np.int64)
+    out["map512_samples"] = uw.ravel()[idx]
+    out["map512_shape"] = np.array(uw.shape)
+    np.savez_compressed(os.path.join(HERE, "unwrap.npz"), **out)
+
+
+ALL = ("projections", "projections_large", "trajectories", "seeds", "helpers", "coherence",
+       "quality", "coherence_opt", "unwraps")
+
 if __name__ == "__main__":
-    projections()
-    projections_large()
-    trajectories()
-    seeds()
-    helpers()
-    coherence()
-    quality()
-    coherence_opt()
+    # make_golden.py <reference root> [fixture function ...] (default: all)
+    for name in (sys.argv[2:] or ALL):
+        globals()[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -13,8 +13,14 @@ import re
 import sys
 import types
 
-REF_ROOT = os.environ.get("SPECKLE_REF_ROOT", "/root/reference")
-PKG = os.path.join(REF_ROOT, "speckle")
+def _pkg_dir():
+    """The reference's ``speckle`` package folder, from ``SPECKLE_REF_ROOT``
+    (the root of a dhparks/als_speckle checkout or install)."""
+    root = os.environ.get("SPECKLE_REF_ROOT")
+    if not root:
+        raise RuntimeError("set SPECKLE_REF_ROOT to the reference checkout (or pass it to "
+                           "make_golden.py)")
+    return os.path.join(root, "speckle")
 
 _PRINT_RE = re.compile(r"^(\s*)print\s+(?!\()(.*)$")
 _EXCEPT_RE = re.compile(r"^(\s*)except\s+([\w.]+)\s*,\s*(\w+)\s*:")
@@ -44,7 +50,7 @@ def _package():
     pkg = sys.modules.get("speckle")
     if pkg is None or not getattr(pkg, "__refshim__", False):
         pkg = types.ModuleType("speckle")
-        pkg.__path__ = [PKG]
+        pkg.__path__ = [_pkg_dir()]
         pkg.__refshim__ = True
         sys.modules["speckle"] = pkg
         # speckle.io needs pyfits (absent); the phasing path only uses it for
@@ -61,7 +67,7 @@ def _load(name, fixups=()):
     full = "speckle." + name
     if full in sys.modules and getattr(sys.modules[full], "__refshim__", False):
         return sys.modules[full]
-    path = os.path.join(PKG, name + ".py")
+    path = os.path.join(_pkg_dir(), name + ".py")
     with open(path) as f:
         src = _py3_text(f.read())
     for a, b in fixups:
@@ -85,7 +91,11 @@ def load_reference():
         warnings.simplefilter("ignore", SyntaxWarning)
         shape = _load("shape")
         masking = _load("masking")
-        wrapping = _load("wrapping")
+        # wrapping.py:161 shapes the unwrapped rows with len/(R-r), a float
+        # that Python 2's numpy truncated and Python 3's rejects
+        wrapping = _load("wrapping", fixups=[
+            ("uw.shape = (R-r, len(plan[0])/(R-r))",
+             "uw.shape = (int(R-r), int(len(plan[0])/(R-r)))")])
         _load("averaging")
         gpu = _load("gpu")
         # crosscorr.py:557-566 relies on Python-2 integer division
@@ -100,8 +110,11 @@ def load_reference():
         conditioning = _load("conditioning", fixups=[
             ("if region != None:", "if region is not None:"),
             ("if align_to == None:", "if align_to is None:")])
+        # phasing.py:1456, :1514, :1604, :1703 pass (0, N/2, (N/2, N/2)) with
+        # Python-2 integer division
         phasing = _load("phasing", fixups=[("import wrapping, masking, gpu, sys, time, io",
-                                            "import wrapping, masking, gpu, sys, time")])
+                                            "import wrapping, masking, gpu, sys, time"),
+                                           ("(0, N/2, (N/2, N/2))", "(0, N//2, (N//2, N//2))")])
     return types.SimpleNamespace(shape=shape, masking=masking, wrapping=wrapping,
                                  gpu=gpu, crosscorr=crosscorr,
                                  conditioning=conditioning, phasing=phasing)

@@ -49,7 +49,7 @@ def test_gpu_rftf_vs_oracle(qual, with_ipsf):
     out, q = gpu_rftf(None, ests, g, ipsf=ip if with_ipsf else None, rftfq=True)
     want = O.gpu_rftf(ests, g, ipsf=ip if with_ipsf else None)
     assert np.max(np.abs(out - want)) < 1e-4
-    assert np.allclose(q, O.annular_average(want), atol=1e-4)
+    assert np.allclose(q, O.unwrap_average(want), atol=1e-4)
 
 
 def test_covar_results_vs_oracle():
