@@ -96,6 +96,9 @@ _SIGS = {
     "sp_com_sums": ([_p, _i, _i, _i, _p, _p], _i),
     "sp_roll_accumulate": ([_p, _i, _i, _i, _p, _p, _p], _i),
     "sp_plain_iterate": ([_i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _p], _i),
+    "sp_unwrap": ([_p, _i, _i, _i, _d, _d, _i, _p, _p, _p, _p], _i),
+    "sp_register_workspace_size": ([_i, _i, _i, C.POINTER(_sz)], _i),
+    "sp_register_subpixel": ([_p, _i, _i, _i, _p, _i, _i, _p, _sz, _p, _p, _p], _i),
     "sp_abs2_f2_f2": ([_p, _p, _i64, _p], _i),
     "sp_sqrt_f2": ([_p, _p, _i64, _p], _i),
     "sp_sqrt_abs_f2": ([_p, _p, _i64, _p], _i),

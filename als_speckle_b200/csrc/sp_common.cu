@@ -18,20 +18,51 @@ void set_error(const char* fmt, ...) {
 }
 
 // Twiddle tables live in a file-scope device array: 64 KiB per device,
-// uploaded once per device by cudaMemcpyToSymbol; nothing is allocated.
+// uploaded once per CUDA context by cudaMemcpyToSymbol; nothing is allocated.
 __device__ __align__(256) float2 g_twiddle[2 * kMaxN];
 
+// Identity of the calling thread's current CUDA context, unique over the
+// life of the process (cuCtxGetId), reached through the runtime's driver
+// entry points so the library does not link libcuda.  0 if unavailable.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0)
+    return 0;
+  return id;
+}
+
+// The tables are uploaded once per CUDA context (a context that is destroyed
+// and created again, e.g. after cudaDeviceReset, gets a fresh module and is
+// uploaded again); the address is looked up on every call.
 static std::mutex g_tw_mutex;
-static bool g_tw_ready[256];
-static const float2* g_tw_addr[256];
+static std::vector<unsigned long long> g_tw_contexts;
 
 cudaError_t twiddles(const float2** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_twiddle);  // also creates the context if needed
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_tw_mutex);
-  if (!g_tw_ready[dev]) {
+  bool ready = false;
+  for (unsigned long long c : g_tw_contexts) ready = ready || (ctx != 0 && c == ctx);
+  if (!ready) {
     std::vector<float2> host(2 * kMaxN, make_float2(0.f, 0.f));
     for (int N = 2; N <= kMaxN; N *= 2) {
       for (int x = 0; x < N; ++x) {
@@ -42,13 +73,9 @@ cudaError_t twiddles(const float2** out) {
     }
     e = cudaMemcpyToSymbol(g_twiddle, host.data(), sizeof(float2) * host.size());
     if (e != cudaSuccess) return e;
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_twiddle);
-    if (e != cudaSuccess) return e;
-    g_tw_addr[dev] = static_cast<const float2*>(p);
-    g_tw_ready[dev] = true;
+    if (ctx != 0) g_tw_contexts.push_back(ctx);
   }
-  *out = g_tw_addr[dev];
+  *out = static_cast<const float2*>(p);
   return cudaSuccess;
 }
 

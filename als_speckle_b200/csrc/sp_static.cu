@@ -10,11 +10,13 @@
 // point takes its scratch from a fixed array in device memory that belongs to
 // this library, and never allocates.
 //
-// The array is kStaticScratchBytes (48 MiB).  Every GPU that loads the library
-// holds it until the process exits.  Requests whose workspace would exceed it
+// The array is kStaticScratchBytes (48 MiB).  A device holds it from the
+// moment this library's device code is loaded there -- at the latest the
+// first sp_engine_run_static call on that device (with CUDA's default lazy
+// module loading), at library load with CUDA_MODULE_LOADING=EAGER -- until
+// the process exits.  Requests whose workspace would exceed it
 // are rejected with SP_ERR_SIZE before any work is enqueued.
 #include <cstring>
-#include <mutex>
 
 #include "sp_common.cuh"
 
@@ -23,29 +25,15 @@ namespace sp {
 constexpr size_t kStaticScratchBytes = (size_t)48 << 20;
 
 // The scratch itself.  Host code must not use this name as an address: on the
-// host it is only a stand-in, so its device address is looked up once per
-// device with cudaGetSymbolAddress and that pointer is what gets passed on.
+// host it is only a stand-in, so its device address is looked up with
+// cudaGetSymbolAddress and that pointer is what gets passed on.
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-static std::mutex g_static_mutex;
-static void* g_static_addr[256];
-
-// Device address of g_static_scratch on the current device (set up on the
-// first call for each device).
+// Device address of g_static_scratch in the current context, looked up on
+// every call (cheap beside an engine run; a cached address would outlive a
+// context that is reset and created again).
 static cudaError_t static_scratch(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (g_static_addr[dev] == nullptr) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) return e;
-    g_static_addr[dev] = p;
-  }
-  *out = g_static_addr[dev];
-  return cudaSuccess;
+  return cudaGetSymbolAddress(out, g_static_scratch);
 }
 
 }  // namespace sp

@@ -441,8 +441,7 @@ def prtf(estimates, N=None, silent=True, prtfq=False):
     call("sp_prtf", ptr(t), F, r, c, N, ptr(work), ptr(out), stream_ptr())
     res = out.cpu().numpy() if was_np else out
     if prtfq:
-        arr = out.cpu().numpy()
-        return res, _annular_average(arr)
+        return res, unwrap_average(out, as_numpy=was_np)
     return res
 
 
@@ -451,18 +450,22 @@ def gpu_prtf(gpuinfo, estimates, N=None, prtfq=False):
     return prtf(estimates, N=N, prtfq=prtfq)
 
 
-def _annular_average(arr):
-    """Average of ``arr`` over unit-width annuli about the centre (N/2, N/2),
-    radii 0..N/2-1: the ``prtfq`` output (reference: polar unwrap with
-    cubic interpolation then a row mean, ``phasing.py:1455-1458``)."""
-    N = arr.shape[0]
-    y, x = np.indices(arr.shape)
-    r = np.hypot(y - N // 2, x - N // 2)
-    ri = np.floor(r).astype(int)
-    keep = ri < N // 2
-    s = np.bincount(ri[keep], weights=arr[keep], minlength=N // 2)
-    n = np.bincount(ri[keep], minlength=N // 2)
-    return s / np.maximum(n, 1)
+def unwrap_average(arr, as_numpy=True):
+    """Azimuthal average of an N x N float map about (N/2, N/2) at radii
+    0 .. N/2 - 1: ``np.average(wrapping.unwrap(arr, (0, N/2, (N/2, N/2))),
+    axis=1)`` (``phasing.py:1454-1458``; ``wrapping.py:8-67``, ``:131-176``),
+    the polar samples taken by cubic B-spline interpolation on the device
+    (``sp_unwrap``).  Returns float32 (numpy if ``as_numpy``)."""
+    a = torch.from_numpy(np.ascontiguousarray(arr, np.float32)).cuda() \
+        if isinstance(arr, np.ndarray) else arr.to(torch.float32).contiguous()
+    if a.dim() != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("unwrap_average needs a square 2d map")
+    N = int(a.shape[0])
+    work = torch.empty((N, N), dtype=torch.float64, device=a.device)
+    mean = torch.empty(N // 2, dtype=torch.float32, device=a.device)
+    call("sp_unwrap", ptr(a), N, 0, N // 2, float(N // 2), float(N // 2), 0, ptr(work), None,
+         ptr(mean), stream_ptr())
+    return mean.cpu().numpy() if as_numpy else mean
 
 
 def _gaussian_1d_kernel(n, sigma):
@@ -544,6 +547,45 @@ def align_frames_device(frames, align_to, use_mag_only=False):
     return out[0] if single else out
 
 
+def align_frames_subpixel(data, align_to=None, upsample=64, return_type="data"):
+    """Align frames to ``align_to`` (default: the first frame) by subpixel
+    shifts and a global phase: the cross-correlation convention and
+    whole-pixel answers of ``conditioning.align_frames``
+    (``conditioning.py:316-430``, ``crosscorr.py:526-568``), refined to
+    1/``upsample`` pixel by the upsampled DFT of Guizar-Sicairos et al. (2008)
+    and applied as a Fourier shift (``sp_register_subpixel``).  The reference
+    aligns by whole pixels only; this is the batched workload's "align to
+    trial 0".  ``return_type``: ``"data"`` (aligned frames, same shape and
+    kind as ``data``), ``"coordinates"`` ((F, 3) array of dy, dx, theta) or
+    ``"both"``."""
+    t, was_np, was2d = _device_frames(data)
+    F, rows, cols = t.shape
+    if align_to is None:
+        ref = t[0].contiguous()
+    else:
+        r, _, r2d = _device_frames(align_to)
+        if not r2d or tuple(r.shape[1:]) != (rows, cols):
+            raise ValueError("align_to must be one frame of the data's shape")
+        ref = r[0].contiguous()
+    N = 1 << (max(rows, cols) - 1).bit_length()
+    N = max(N, 8)
+    nbytes = C.c_size_t(0)
+    call("sp_register_workspace_size", F, N, int(upsample), C.byref(nbytes))
+    work = torch.empty(nbytes.value, dtype=torch.uint8, device=t.device)
+    shifts = torch.empty((F, 3), dtype=torch.float64, device=t.device)
+    out = torch.empty_like(t) if return_type != "coordinates" else None
+    call("sp_register_subpixel", ptr(t), F, rows, cols, ptr(ref), N, int(upsample), ptr(work),
+         nbytes.value, ptr(shifts), ptr(out), stream_ptr())
+    coords = shifts.cpu().numpy() if was_np else shifts
+    if return_type == "coordinates":
+        return coords[0] if was2d else coords
+    o = out[0] if was2d else out
+    o = o.cpu().numpy() if was_np else o
+    if return_type == "both":
+        return o, (coords[0] if was2d else coords)
+    return o
+
+
 def center_of_mass_average(imgs):
     """Sum of frames rolled so their |img| centres of mass coincide with the
     first frame's (``phasing.py:1710-1745``)."""
@@ -623,7 +665,8 @@ def rftf(estimate, goal_modulus, hot_pixels=False, ipsf=None, rftfq=False, scale
     function does), lined up with the goal (centred at (0,0) or (N/2,N/2),
     whichever fits better), ``sqrt(1/(1+(F-g)^2/g^2))`` in the centred layout,
     optionally rescaled to [0, 1] and cleaned of hot pixels.  N must be a
-    power of two here.  ``rftfq`` adds the annular mean about the centre."""
+    power of two here.  ``rftfq`` adds the polar-unwrapped azimuthal average
+    (``unwrap_average``, ``phasing.py:1603-1605``)."""
     est, was_np, _ = _device_frames(estimate)
     g = torch.from_numpy(np.ascontiguousarray(goal_modulus, np.float32)).cuda() \
         if isinstance(goal_modulus, np.ndarray) else goal_modulus.to(torch.float32).contiguous()
@@ -654,7 +697,7 @@ def rftf(estimate, goal_modulus, hot_pixels=False, ipsf=None, rftfq=False, scale
         _hot_pixels(out, 1.1)
     res = out.cpu().numpy() if was_np else out
     if rftfq:
-        return res, _annular_average(out.cpu().numpy())
+        return res, unwrap_average(out, as_numpy=was_np)
     return res
 
 
@@ -688,7 +731,7 @@ def gpu_rftf(gpuinfo, estimates, goal_modulus, ipsf=None, rftfq=False):
     call("sp_rftf_accumulate", L, ptr(g), ptr(acc), ptr(f), N, 1, st)
     res = acc.cpu().numpy() if was_np else acc
     if rftfq:
-        return res, _annular_average(acc.cpu().numpy())
+        return res, unwrap_average(acc, as_numpy=was_np)
     return res
 
 

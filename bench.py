@@ -34,6 +34,7 @@ TRIALS = 128
 ORDER = (("hio", 500), ("er", 50))
 ITERS = 550
 BETA = 0.9
+UPSAMPLE = 64  # subpixel registration to 1/64 pixel
 BYTES_PER_PX = 24  # algorithmic bytes per trial-iteration per pixel: psi r+w 16, modulus 4, support 4
 METRIC = "HIO trial-iterations/s, 512^2 x 128 trials (500 HIO + 50 ER), batched"
 UNIT = "trial-iter/s"
@@ -150,6 +151,40 @@ def cpu_baseline(max_procs=64, iters=24):
                       "complex64 algorithm (oracle port), %.1f s wall" % (procs, iters, wall)}
 
 
+def _fp64_worker(args):
+    """One trial of the benchmark job (same random-phase start) iterated in
+    FP64 by the oracle, cropped: the checker of the FP32 average."""
+    seed, trial, box = args
+    from als_speckle_b200 import synth
+    from oracle import phasing_oracle as O
+    obj, M, S = synth.config_pattern("hio_512x128", seed=0)
+    psi = O.seed_random_phase(M, S, seed, trial, mode="f64")
+    psi = O.iterate(psi, M, S, ITERS, order=ORDER, beta=BETA, quirks="gpu", mode="f64")
+    r0, c0, rows, cols = box
+    return psi[r0:r0 + rows, c0:c0 + cols]
+
+
+def fp64_average_error(job, trials=4):
+    """Relative L2 error of the device's averaged reconstruction of the job's
+    first ``trials`` trials (FP32 iterates, aligned to trial 0) against the
+    same trials from the same starts run, aligned and averaged in FP64 by the
+    oracle (spawned processes, one trial each; part of the CPU-baseline leg)."""
+    import multiprocessing as mp
+    from oracle import phasing_oracle as O
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(trials) as pool:
+        frames = pool.map(_fp64_worker, [(job.seed, k, job.box) for k in range(trials)])
+    f64 = O.align_global_phase(np.stack(frames))
+    _, f64 = O.register_subpixel(f64, f64[0], N=job.reg_n, upsample=UPSAMPLE)
+    avg64 = f64.mean(axis=0)
+    avg32 = job.save[:trials].cpu().numpy().astype(np.complex128).mean(axis=0)
+    err = float(np.linalg.norm(avg32 - avg64) / np.linalg.norm(avg64))
+    return {"value": err, "trials": trials, "seconds": round(time.perf_counter() - t0, 1),
+            "what": "||avg_fp32 - avg_fp64|| / ||avg_fp64|| of the first %d trials, both aligned to "
+                    "trial 0 (global phase + subpixel shift) after 500 HIO + 50 ER from the same "
+                    "starts; FP64 = the oracle" % trials}
+
+
 # ------------------------------------------------------------ GPU side
 def build_inputs(torch, device):
     from als_speckle_b200 import synth
@@ -185,6 +220,15 @@ class Job:
         self.avg = torch.empty((rows, cols), dtype=torch.complex64, device=device)
         self.sums = torch.empty(5 * TRIALS, dtype=torch.float64, device=device)
         self.angles = torch.empty(TRIALS, dtype=torch.float64, device=device)
+        # subpixel registration to trial 0: crops in the next power-of-two transform
+        from als_speckle_b200._lib import call
+        import ctypes
+        self.reg_n = 1 << (max(rows, cols) - 1).bit_length()
+        nb = ctypes.c_size_t(0)
+        call("sp_register_workspace_size", TRIALS, self.reg_n, UPSAMPLE, ctypes.byref(nb))
+        self.reg_bytes = nb.value
+        self.reg_work = torch.empty(nb.value, dtype=torch.uint8, device=device)
+        self.shifts = torch.empty((TRIALS, 3), dtype=torch.float64, device=device)
         self.launches = 0
 
     def step(self):
@@ -195,10 +239,16 @@ class Job:
         s = stream_ptr()
         call("sp_align_global_phase", ptr(self.save), TRIALS, rows * cols, ptr(self.angles),
              ptr(self.sums), s)
+        # subpixel shift and global phase of every trial onto trial 0, in place
+        call("sp_register_subpixel", ptr(self.save), TRIALS, rows, cols, ptr(self.save[0]),
+             self.reg_n, UPSAMPLE, ptr(self.reg_work), self.reg_bytes, ptr(self.shifts),
+             ptr(self.save), s)
         call("sp_mean_frames", ptr(self.save), TRIALS, rows * cols, ptr(self.avg), s)
         call("sp_prtf", ptr(self.save), TRIALS, rows, cols, N, ptr(self.prtf_work), ptr(self.prtf), s)
-        # align: 2 kernels, mean: 1, prtf: embed + 2 FFT passes + accumulate
-        self.launches = eng + 2 + 1 + 4
+        # align: 2 kernels; register: 2 embeds, 3 two-pass FFTs, cross, argmax,
+        # table, 2 upsampled DFTs, finish, shift, crop; mean: 1; prtf: embed +
+        # 2 FFT passes + accumulate
+        self.launches = eng + 2 + 16 + 1 + 4
 
     def r_factor(self):
         m = self.M.double()
@@ -347,6 +397,7 @@ def run_ours(args):
     }
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+        line["avg_err_vs_fp64"] = fp64_average_error(job)
     print(json.dumps(line))
 
 
@@ -365,7 +416,8 @@ def run_e2e(torch, device, M, S, args, engine, sync=None):
     """Same job through the phasing API with host buffers every step.  Under
     torchrun every rank runs its own job; ``sync`` (a barrier) lines the ranks
     up before the timed loop and the caller takes the slowest rank's time."""
-    from als_speckle_b200.phasing import phasing, align_global_phase, prtf, mean_frames
+    from als_speckle_b200.phasing import (phasing, align_global_phase, align_frames_subpixel, prtf,
+                                          mean_frames)
     Mh = torch.from_numpy(M).pin_memory()
     Sh = torch.from_numpy(S).pin_memory()
     r = phasing(device=device, engine=engine)
@@ -375,7 +427,7 @@ def run_e2e(torch, device, M, S, args, engine, sync=None):
         r.load(modulus=Mh.numpy(), support=Sh.numpy(), numtrials=TRIALS)
         psis, errs = r.iterate_trials(ITERS, TRIALS, order=ORDER, beta=BETA, seed=7, errors=True)
         sb = r.savebuffer[:TRIALS]
-        al = align_global_phase(sb)
+        al = align_frames_subpixel(align_global_phase(sb), upsample=UPSAMPLE)
         avg = mean_frames(al).cpu()
         p = prtf(al, N=N).cpu()
         rf = errs[:, -1, 1].cpu()
@@ -394,7 +446,8 @@ def run_e2e(torch, device, M, S, args, engine, sync=None):
     dt = time.perf_counter() - t0
     return {"value": TRIALS * ITERS * args.steps / dt, "unit": UNIT,
             "h2d_bytes_per_step": int(M.nbytes + S.nbytes), "d2h_bytes_per_step": int(d2h),
-            "api": "phasing.load + iterate_trials + align_global_phase + mean_frames + prtf",
+            "api": "phasing.load + iterate_trials + align_global_phase + align_frames_subpixel + "
+                   "mean_frames + prtf",
             "seconds": dt}
 
 

@@ -124,10 +124,14 @@ int64_t sp_engine_last_launches(void);
  * with no access to an allocator, or code that must not allocate once it is
  * running).  No counterpart in the reference, which allocates its buffers in
  * phasing.load.  Scratch comes from a 48 MiB array in device memory owned by
- * this library, which every GPU that loads the library holds until exit;
- * requests needing more (sp_engine_workspace_size) fail with SP_ERR_SIZE.
- * The first call on each device looks up the array's address; make that first
- * call before any stream capture.  All calls share the array, so calls that
+ * this library; a device reserves it when the library's device code is
+ * loaded there -- at the latest on the first sp_engine_run_static call on
+ * that device (lazy module loading, CUDA's default), at library load with
+ * CUDA_MODULE_LOADING=EAGER -- and holds it until the process exits.
+ * Requests needing more (sp_engine_workspace_size) fail with SP_ERR_SIZE.
+ * Each call looks up the array's address in the current context (the first
+ * lookup on a device may load the module); make the first call on each
+ * device before any stream capture.  All calls share the array, so calls that
  * overlap on the GPU (other streams, other threads) race; nothing in it needs
  * to start at zero.  Launches are eager (opts->use_graph is ignored). */
 int sp_engine_run_static(const sp_trial* trials, int n_trials, const sp_run_opts* opts,
@@ -213,6 +217,38 @@ int sp_com_sums(const void* frames_dev, int n_frames, int rows, int cols, double
 /* ... then out = sum_n roll(frame_n, -shift_n) with shifts_dev = (dr, dc) per frame. */
 int sp_roll_accumulate(const void* frames_dev, int n_frames, int rows, int cols,
                        const int* shifts_dev, void* out_dev, sp_stream_t stream);
+
+/* Subpixel registration and alignment of frames to a reference (the batched
+ * workload's "align to trial 0, then average"; the reference itself aligns
+ * by whole pixels only: conditioning.align_frames :316-430 with
+ * crosscorr.alignment_coordinates :526-568, whose correlation convention and
+ * whole-pixel answers this keeps).  Frames (n_frames, rows, cols) and the
+ * reference (rows, cols) are embedded at the corner of N x N (N a power of
+ * two >= rows, cols); the cross-correlation peak is refined by the
+ * upsampled DFT of Guizar-Sicairos, Thurman & Fienup (Opt. Lett. 33, 2008) to
+ * 1/upsample pixel (1..170).  shifts_dev receives (dy, dx, theta) per frame
+ * (3 doubles): frame_f(y + d) exp(-i theta) lines up with the reference.  If
+ * out_dev is not NULL it receives those aligned frames (Fourier-shifted,
+ * cropped to rows x cols; may equal frames_dev).  work_dev:
+ * sp_register_workspace_size bytes. */
+int sp_register_workspace_size(int n_frames, int N, int upsample, size_t* bytes);
+int sp_register_subpixel(const void* frames_dev, int n_frames, int rows, int cols,
+                         const void* ref_dev, int N, int upsample, void* work_dev,
+                         size_t work_bytes, double* shifts_dev, void* out_dev, sp_stream_t stream);
+
+/* Polar unwrap of an N x N float map and its row means: the prtfq / rftfq
+ * azimuthal averages (phasing.py:1454-1458, :1512-1516, :1603-1605,
+ * :1701-1705), which call wrapping.unwrap(map, (0, N/2, (N/2, N/2)))
+ * (wrapping.py:8-67 unwrap_plan, :131-176 unwrap) and np.average(axis=1).
+ * Samples radii r_in .. r_out-1 about (cy, cx) at `columns` angles
+ * 2 pi k / columns (columns <= 0: int(2 pi r_out)), each by cubic B-spline
+ * interpolation in FP64 (scipy.ndimage.map_coordinates order 3: mirror-
+ * boundary prefilter) rounded to float; every sample must lie inside the map
+ * (SP_ERR_INVALID otherwise).  unwrapped_dev ((r_out - r_in) x columns
+ * floats) and mean_dev (r_out - r_in floats) may each be NULL, not both.
+ * work_dev: N*N doubles. */
+int sp_unwrap(const float* in_dev, int N, int r_in, int r_out, double cy, double cx, int columns,
+              double* work_dev, float* unwrapped_dev, float* mean_dev, sp_stream_t stream);
 
 /* ---- trial quality: RFTF, hot pixels, pair-wise covariances ------------- */
 /* (|x|^2, 0)  -- kernels/common_abs2_f2_f2.cl */

@@ -4,7 +4,9 @@ It serves callers that cannot allocate device memory themselves (a host
 framework that owns all allocations, a plugin without an allocator): its
 scratch is a fixed 48 MiB array inside the library.  These tests call it
 through the C ABI and check that two calls in a row give what
-sp_engine_run gives with a caller-allocated workspace, to the engine's
+sp_engine_run gives with a caller-allocated workspace -- coherent trials of
+several sizes and algorithms, and partially coherent ones (ipsf, energy
+spectrum) -- to the engine's
 single-projection tolerance (1e-5 relative L2 norm) -- in practice bit for bit.
 """
 import ctypes as C
@@ -17,17 +19,30 @@ pytestmark = pytest.mark.gpu
 
 
 def _trials(seed=0):
-    """A small mixed batch: sizes, algorithms and starts differ per trial."""
+    """A small mixed batch: sizes, algorithms and starts differ per trial;
+    the last two project partially coherently (an ipsf, and an energy
+    spectrum with an ipsf), which adds divisor planes and a job table to the
+    scratch layout."""
     from als_speckle_b200 import synth
-    from als_speckle_b200.engine import TrialSpec
+    from als_speckle_b200.workloads import gaussian_ipsf
     out = []
-    for k, (N, order, iters) in enumerate(((256, (("hio", 6), ("er", 2)), 8),
-                                           (512, (("raar", 5),), 5),
-                                           (128, (("dm", 3), ("er", 1)), 4))):
+    for k, (N, order, iters, coh) in enumerate(((256, (("hio", 6), ("er", 2)), 8, None),
+                                                (512, (("raar", 5),), 5, None),
+                                                (128, (("dm", 3), ("er", 1)), 4, None),
+                                                (128, (("hio", 3), ("dm", 2)), 5, "ipsf"),
+                                                (64, (("raar", 4),), 4, "spectrum"))):
         _, M, S = synth.pattern(N, n_ellipses=5, box=N // 4, peak=1e6, seed=seed + k,
                                 support_edge=N // 4 + 8)
-        out.append(dict(N=N, order=order, iters=iters, M=torch.from_numpy(M).cuda(),
-                        S=torch.from_numpy(S).cuda(), trial=k))
+        d = dict(N=N, order=order, iters=iters, M=torch.from_numpy(M).cuda(),
+                 S=torch.from_numpy(S).cuda(), trial=k, ipsf=None, spectrum=None)
+        if coh is not None:
+            d["ipsf"] = torch.from_numpy(gaussian_ipsf(N, 1.5)).cuda()
+        if coh == "spectrum":
+            e = np.linspace(0.96, 1.04, 5)
+            w = np.exp(-0.5 * np.linspace(-2, 2, 5) ** 2)
+            d["spectrum"] = (torch.from_numpy((e / e[2]).astype(np.float32)).cuda(),
+                             torch.from_numpy(w.astype(np.float32)).cuda())
+        out.append(d)
     return out
 
 
@@ -36,7 +51,7 @@ def _specs(inp, psis, saves, errs):
     return [TrialSpec(psi=psis[k], modulus=d["M"], support=d["S"], iterations=d["iters"],
                       order=d["order"], beta=0.9, random_phase=True, seed=5, trial=d["trial"],
                       box=(d["N"] // 4, d["N"] // 4, d["N"] // 2, d["N"] // 2), save=saves[k],
-                      errors=errs[k])
+                      errors=errs[k], ipsf=d["ipsf"], spectrum=d["spectrum"])
             for k, d in enumerate(inp)]
 
 
