@@ -571,6 +571,11 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
 
 extern "C" int64_t sp_engine_last_launches(void) { return g_last_launches; }
 
+extern "C" int64_t sp_engine_graph_count(void) {
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  return (int64_t)g_graphs.size();
+}
+
 extern "C" int sp_engine_release_graphs(void) {
   std::lock_guard<std::mutex> lock(g_graph_mutex);
   for (auto& kv : g_graphs) cudaGraphExecDestroy(kv.second);

@@ -128,12 +128,18 @@ class ServingEngine:
     """Admit requests against ``hbm_budget`` bytes and advance them in rounds
     of up to ``chunk`` iterations (continuous batching)."""
 
+    # cached launch graphs kept before the service drops them (each active set
+    # of requests has its own launch shape, hence its own graph)
+    MAX_GRAPHS = 32
+
     def __init__(self, device=None, hbm_budget=120 << 30, chunk=64, engine: Engine = None,
-                 max_active_trials=4096):
+                 max_active_trials=4096, use_graph=True):
         self.device = torch.device(device if device is not None else "cuda")
         self.budget = int(hbm_budget)
         self.chunk = int(chunk)
-        self.engine = engine or Engine(device=self.device, use_graph=False)
+        # rounds whose active set did not change replay the previous round's
+        # CUDA graph (one launch for the round's 2 x chunk kernels)
+        self.engine = engine or Engine(device=self.device, use_graph=use_graph)
         self.max_active_trials = max_active_trials
         self.pending: List = []     # heap of (arrival, rid, request)
         self.active: List[_Active] = []
@@ -145,10 +151,6 @@ class ServingEngine:
 
     def _on_stream(self):
         return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
-
-    def _sync(self):
-        if self.stream is not None:
-            self.stream.synchronize()
 
     def submit(self, req: Request):
         """Queue a request.  Rejected at once: a request larger than the
@@ -220,13 +222,23 @@ class ServingEngine:
                 self.trial_iterations += n * a.req.trials
             with self._on_stream():
                 self.engine.solve(specs, stream=self.stream)
-            self._sync()
+                # one device-side finiteness flag per request, read back in a
+                # single copy (the round's only host synchronisation)
+                flags = torch.stack([torch.isfinite(a.errors[:, a.done + n - 1]).all() if n else
+                                     torch.ones((), dtype=torch.bool, device=self.device)
+                                     for a, n in zip(self.active, steps)])
+                finite = flags.cpu().tolist()
+            # the stream is idle here (the flags were read back): a safe point
+            # to drop cached graphs of launch shapes that have come and gone
+            if getattr(self.engine, "use_graph", False) and \
+                    _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
+                _lib.call("sp_engine_release_graphs")
             self.rounds += 1
             t = (clock() - t0)
             still = []
-            for a, n in zip(self.active, steps):
+            for a, n, ok in zip(self.active, steps, finite):
                 a.done += n
-                if n and not bool(torch.isfinite(a.errors[:, a.done - 1]).all()):
+                if n and not ok:
                     # the iterate has become non-finite: stop it and free its slots
                     self.results[a.req.rid] = Result(
                         a.req.rid, a.save.cpu().numpy(), a.errors.cpu().numpy(), a.box,

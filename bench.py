@@ -9,7 +9,9 @@ on the device.  The metric is trial-iterations per second over the job.
 
 Under torchrun each rank runs its own 128-trial job (weak scaling, no
 collective on the data path); the printed value is the sum over ranks
-divided by the slowest rank's time.
+divided by the slowest rank's time.  ``--mode strong`` instead splits one
+128-trial job over the ranks (distributed.solve_sharded: one broadcast and
+two all-reduces after the iterations).
 """
 from __future__ import annotations
 
@@ -255,6 +257,35 @@ class Job:
         return (self.errs[:, -1, 1] / m.sum()).cpu().numpy()
 
 
+class ShardedJob:
+    """The same 128-trial job split across the ranks (strong scaling):
+    ``distributed.solve_sharded`` -- each rank iterates its share, trial 0's
+    owner broadcasts its phase-aligned crop, every rank registers to it, and
+    the frame and PRTF-phasor sums are all-reduced before the average and
+    the PRTF are finished."""
+
+    def __init__(self, torch, device, M, S, box, engine, seed):
+        from als_speckle_b200.distributed import DeviceOps
+        self.M = torch.from_numpy(M).to(device)
+        self.S = torch.from_numpy(S).to(device)
+        self.box = box
+        self.seed = seed
+        self.ops = DeviceOps(engine=engine)
+        self.launches = 0
+        self.mine = []
+
+    def step(self):
+        from als_speckle_b200._lib import lib
+        from als_speckle_b200.distributed import solve_sharded
+        self.avg, self.prtf, count, self.mine = solve_sharded(
+            self.M, self.S, TRIALS, ITERS, order=ORDER, beta=BETA, seed=self.seed, box=self.box,
+            N_prtf=N, upsample=UPSAMPLE, ops=self.ops)
+        self.launches = int(lib.sp_engine_last_launches()) + 2 + 16 + 1 + 5
+
+    def r_factor(self):
+        return np.array([float("nan")])
+
+
 def flush_l2(torch, buf):
     buf.fill_(1)
 
@@ -313,7 +344,9 @@ def run_ours(args):
     engine = Engine(device=device, use_graph=True, l2_group_bytes=tune["l2_group_bytes"],
                     e_per_n={N: tune["E"]})
     M, S, box = build_inputs(torch, device)
-    job = Job(torch, device, M, S, box, engine, seed=1000 + rank)
+    strong = args.mode == "strong"
+    job = ShardedJob(torch, device, M, S, box, engine, seed=1000) if strong else \
+        Job(torch, device, M, S, box, engine, seed=1000 + rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # 256 MiB > L2
 
     def barrier():
@@ -345,7 +378,8 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_s = float(t.item())
-    work = TRIALS * ITERS * world * args.steps
+    # replicas: every rank runs a whole job; strong: the ranks share one job
+    work = TRIALS * ITERS * (1 if strong else world) * args.steps
     value = work / total_s
     launches = job.launches * args.steps
     rfac = job.r_factor()
@@ -358,11 +392,13 @@ def run_ours(args):
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e["value"] = TRIALS * ITERS * args.steps * world / float(et.item())
     # kernel-level roofline: one steady iteration tick of one L2 group
-    per_tick, group = kernel_pass_times(torch, engine, job)
+    per_tick, group = kernel_pass_times(
+        torch, engine, Job(torch, device, M, S, box, engine, seed=1000) if strong else job)
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_PX * N * N * group / per_tick / 1e9
     plain = run_plain(torch, device, M, S)
     single = run_single_trial(torch, device, M, S, engine)
+    serving = run_serving() if world == 1 and args.serving else None
 
     if world > 1:
         dist.barrier()
@@ -372,11 +408,13 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "higher_is_better": True, "scaling": "strong" if strong else "weak",
+        "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (seeded ellipse objects, Poisson noise; reference example data unavailable)",
         "config": {"workload": WORKLOAD, "trials": TRIALS, "iterations": "500 hio + 50 er",
                    "beta": BETA, "l2": "inputs larger than L2 (512 MiB psi+G per job) and a "
-                   "256 MiB L2 flush before every step", "parallelism": "replicas x%d" % world,
+                   "256 MiB L2 flush before every step", "parallelism": ("trial-sharded x%d (one job)" % world) if strong
+                   else "replicas x%d" % world,
                    "E": tune["E"], "l2_group_bytes": tune["l2_group_bytes"]},
         "latency_ms": {"p50": 1e3 * float(np.percentile(step_s, 50)),
                        "p99": 1e3 * float(np.percentile(step_s, 99))},
@@ -393,11 +431,15 @@ def run_ours(args):
         "plain_gpu": plain,
         "single_trial_engine": single,
         "batched_over_plain": value / world / plain["value"],
+        "batched_over_single_trial_engine": value / world / single["value"],
         "clocks": clk.summary(),
     }
+    if serving is not None:
+        line["serving"] = serving
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
-        line["avg_err_vs_fp64"] = fp64_average_error(job)
+        if not strong:
+            line["avg_err_vs_fp64"] = fp64_average_error(job)
     print(json.dumps(line))
 
 
@@ -500,6 +542,21 @@ def run_single_trial(torch, device, M, S, engine, iters=200):
             "what": "1 trial through the fused engine (CUDA graph)"}
 
 
+def run_serving(rate=4.0, window=5.0):
+    """The continuous-batching service on the mixed request stream (sizes
+    256^2..2048^2 at .4/.3/.2/.1, HIO/ER/RAAR/DM, 200-2000 iterations, 1-16
+    trials) offered at a rate it sustains: p50/p99 request latency (arrival to
+    result on the host) and delivered pixel-iterations per second."""
+    from als_speckle_b200 import workloads
+    r = workloads.serving(rate=rate, window=window, seed=0)
+    keep = ("rate", "window_s", "requests", "wall_s", "p50_latency_s", "p99_latency_s",
+            "gpx_iterations_per_s", "trial_iterations_per_s", "rounds")
+    out = {k: r[k] for k in keep}
+    out["what"] = ("Poisson arrivals, sizes 256^2-2048^2 (.4/.3/.2/.1), HIO/ER/RAAR/DM, 200-2000 "
+                   "iterations, 1-16 trials, 120 GB budget, rounds of 64 iterations")
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -540,6 +597,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-serving", dest="serving", action="store_false")
+    ap.add_argument("--mode", choices=("replicas", "strong"), default="replicas",
+                    help="replicas: one whole job per rank (weak scaling); strong: one job "
+                         "sharded over the ranks")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

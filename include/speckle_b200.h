@@ -115,6 +115,10 @@ int sp_engine_run(const sp_trial* trials, int n_trials, void* workspace_dev,
 /* Destroy the CUDA graphs cached by sp_engine_run (call before freeing a
  * workspace that was used with use_graph = 1). */
 int sp_engine_release_graphs(void);
+/* Number of CUDA graphs sp_engine_run holds in its cache (one per workspace
+ * and launch shape); a long-running caller whose shapes keep changing can
+ * release them (sp_engine_release_graphs) once its stream is idle. */
+int64_t sp_engine_graph_count(void);
 /* Kernel launches enqueued by the calling thread's last sp_engine_run
  * (kernels inside a launched graph count individually). */
 int64_t sp_engine_last_launches(void);

@@ -59,3 +59,33 @@ def test_service_equals_engine_solve():
     torch.cuda.synchronize()
     assert np.array_equal(saves.cpu().numpy(), res.save)
     eng.close()
+
+
+def test_final_r_factor_vs_fp64_oracle():
+    """Requests of the serving mix (sizes, algorithms, trial counts drawn as
+    the service's Poisson workload draws them, shortened so the FP64 oracle
+    finishes in seconds): every trial's final R-factor, sum||F|-M| / sum M of
+    the last iteration, beside the oracle's from the same random-phase start.
+    Tolerance 1e-3 relative (FP32 against FP64 over at most 40 iterations)."""
+    from als_speckle_b200.serving import poisson_workload
+    from oracle import phasing_oracle as O
+    reqs = poisson_workload(n_requests=6, window=10.0, rate=50.0, seed=3, sizes=(64, 128),
+                            probs=(0.5, 0.5), iters=(12, 40), trials=(1, 3), patterns_per_size=1)
+    assert len(reqs) == 6
+    res = _serve(reqs, chunk=16)
+    rows = []
+    for r in reqs:
+        out = res[r.rid]
+        assert out.status == "done"
+        M = r.modulus.astype(np.float32)
+        S = (r.support / r.support.max()).astype(np.float32)
+        for k in range(r.trials):
+            psi = O.seed_random_phase(M, S, r.seed, k, mode="f64")
+            _, errs = O.iterate(psi, M, S, r.iterations, order=r.order, beta=r.beta, mode="f64",
+                                errors=True)
+            want = errs[-1][1]
+            got = out.errors[k, -1, 1] / float(np.sum(M.astype(np.float64)))
+            rows.append((r.rid, r.n, r.order[0][0], r.iterations, k, got, want))
+            assert abs(got - want) <= 1e-3 * want, rows[-1]
+    for row in rows:
+        print("request %d N=%d %s x%d trial %d: R gpu %.6f fp64 %.6f" % row)
