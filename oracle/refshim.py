@@ -1,12 +1,15 @@
 """Load the reference's numpy phasing path under Python 3, read-only.
 
-The reference (dhparks/als_speckle) is Python-2 source.  This loader reads the
-needed modules' text from the reference checkout, applies mechanical
+TEST AND BASELINE INFRASTRUCTURE ONLY.  The reference (dhparks/als_speckle)
+is Python-2 source.  This loader reads the needed modules' text from a
+reference checkout or install (``SPECKLE_REF_ROOT``), applies mechanical
 source-level fixes in memory (print statements, backslash continuations,
-implicit relative imports) and executes them as modules.  Nothing on disk is
-modified.  It exists only to generate the golden fixtures in this folder; the
-tests themselves never import it (the reference is not present where the GPU
-tests run).
+implicit relative imports, Python-2 integer division where the path needs
+it) and executes them as modules.  Nothing on disk is modified.  Users:
+``tests/golden/make_golden.py`` (the golden fixtures) and ``bench.py``'s
+reference arm and CPU baseline, which time the reference's own numpy
+iteration from the install in ``baseline/_ref``.  The product never imports
+it.
 """
 import os
 import re

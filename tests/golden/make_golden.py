@@ -16,10 +16,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 if len(sys.argv) > 1:
     os.environ["SPECKLE_REF_ROOT"] = sys.argv[1]
 import golden_inputs as inputs  # noqa: E402
-import refshim  # noqa: E402
+from oracle import refshim  # noqa: E402
 
 ref = refshim.load_reference()
 
