@@ -229,38 +229,84 @@ def cpu_baseline(iters=24):
             "sample": pool.describe(iters) + ", %.1f s wall" % wall}
 
 
-def _fp64_worker(args):
-    """One trial of the benchmark job (same random-phase start) iterated in
-    FP64 by the oracle, cropped: the checker of the FP32 average."""
-    seed, trial, box = args
+def _precision_worker(args):
+    """One trial of the benchmark job (the same random-phase start) iterated
+    by the oracle in FP64 (mode "f64") or in numpy complex64 (mode "ref64",
+    the reference's CPU arithmetic), cropped: the checkers of the FP32
+    average."""
+    seed, trial, box, mode = args
     from als_speckle_b200 import synth
     from oracle import phasing_oracle as O
     obj, M, S = synth.config_pattern("hio_512x128", seed=0)
-    psi = O.seed_random_phase(M, S, seed, trial, mode="f64")
-    psi = O.iterate(psi, M, S, ITERS, order=ORDER, beta=BETA, quirks="gpu", mode="f64")
+    psi = O.seed_random_phase(M, S, seed, trial, mode=mode)
+    psi = O.iterate(psi, M, S, ITERS, order=ORDER, beta=BETA, quirks="gpu", mode=mode)
     r0, c0, rows, cols = box
-    return psi[r0:r0 + rows, c0:c0 + cols]
+    return np.asarray(psi[r0:r0 + rows, c0:c0 + cols], np.complex128)
 
 
-def fp64_average_error(job, trials=4):
-    """Relative L2 error of the device's averaged reconstruction of the job's
-    first ``trials`` trials (FP32 iterates, aligned to trial 0) against the
-    same trials from the same starts run, aligned and averaged in FP64 by the
-    oracle (spawned processes, one trial each; part of the CPU-baseline leg)."""
+def _truth_error(avg, truth, reg_n):
+    """Relative error of a reconstruction against the true object after
+    registration (subpixel shift), a complex least-squares scale (the
+    global phase and the photon scaling) and the twin ambiguity (the
+    conjugate point-inverted image is an equally valid solution)."""
+    from oracle import phasing_oracle as O
+    best = np.inf
+    for cand in (avg, np.conj(avg[::-1, ::-1])):
+        _, al = O.register_subpixel(cand[None], truth, N=reg_n, upsample=UPSAMPLE)
+        a = al[0]
+        c = np.vdot(truth, a) / np.vdot(truth, truth)
+        best = min(best, float(np.linalg.norm(a - c * truth) / np.linalg.norm(c * truth)))
+    return best
+
+
+def precision_check(job, trials=4):
+    """The averaged reconstruction in FP32 against FP64, on the job's first
+    ``trials`` trials from the same starts (part of the CPU-baseline leg; the
+    oracle runs them in spawned processes).
+
+    * value: ||avg_gpu - avg_fp64|| / ||avg_fp64||, both aligned to trial 0
+      (global phase + subpixel shift) and averaged;
+    * numpy_c64_vs_fp64: the same for the reference's complex64 numpy
+      arithmetic -- HIO iterations are chaotic, so FP32 and FP64 runs from one
+      start drift apart (their R-factor curves differ by ~1e-4 after 50
+      iterations and ~1e-2 after a few hundred) and end at different,
+      equally valid solutions; this figure is that drift for the reference's
+      own precision, the yardstick for the first;
+    * err_vs_truth: each average against the true (synthetic) object after
+      registration, a complex scale and the twin choice -- the precision-
+      independent quality of the result."""
     import multiprocessing as mp
+    from als_speckle_b200 import synth
     from oracle import phasing_oracle as O
     t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(trials) as pool:
-        frames = pool.map(_fp64_worker, [(job.seed, k, job.box) for k in range(trials)])
-    f64 = O.align_global_phase(np.stack(frames))
-    _, f64 = O.register_subpixel(f64, f64[0], N=job.reg_n, upsample=UPSAMPLE)
-    avg64 = f64.mean(axis=0)
-    avg32 = job.save[:trials].cpu().numpy().astype(np.complex128).mean(axis=0)
-    err = float(np.linalg.norm(avg32 - avg64) / np.linalg.norm(avg64))
-    return {"value": err, "trials": trials, "seconds": round(time.perf_counter() - t0, 1),
-            "what": "||avg_fp32 - avg_fp64|| / ||avg_fp64|| of the first %d trials, both aligned to "
-                    "trial 0 (global phase + subpixel shift) after 500 HIO + 50 ER from the same "
-                    "starts; FP64 = the oracle" % trials}
+    args = [(job.seed, k, job.box, mode) for mode in ("f64", "ref64") for k in range(trials)]
+    with mp.get_context("spawn").Pool(len(args)) as pool:
+        frames = pool.map(_precision_worker, args)
+    f64, c64 = np.stack(frames[:trials]), np.stack(frames[trials:])
+
+    def average(fr):
+        fr = O.align_global_phase(fr)
+        _, fr = O.register_subpixel(fr, fr[0], N=job.reg_n, upsample=UPSAMPLE)
+        return fr.mean(axis=0)
+
+    avg64, avgc64 = average(f64), average(c64)
+    save = job.save.cpu().numpy().astype(np.complex128)  # aligned to trial 0 already
+    avg32 = save[:trials].mean(axis=0)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    obj, _, _ = synth.config_pattern("hio_512x128", seed=0)
+    r0, c0, rows, cols = job.box
+    truth = np.asarray(obj[r0:r0 + rows, c0:c0 + cols], np.complex128)
+    return {"value": rel(avg32, avg64), "trials": trials,
+            "numpy_c64_vs_fp64": rel(avgc64, avg64),
+            "err_vs_truth": {"gpu_fp32_all_%d" % TRIALS: _truth_error(save.mean(axis=0), truth, job.reg_n),
+                             "gpu_fp32": _truth_error(avg32, truth, job.reg_n),
+                             "fp64": _truth_error(avg64, truth, job.reg_n),
+                             "numpy_c64": _truth_error(avgc64, truth, job.reg_n)},
+            "seconds": round(time.perf_counter() - t0, 1),
+            "what": "average of the first %d trials (500 HIO + 50 ER from the same starts, aligned "
+                    "to trial 0): GPU FP32 vs the oracle's FP64 (value) and numpy complex64 vs FP64; "
+                    "errors against the true object after registration, complex scale and twin "
+                    "choice" % trials}
 
 
 # ------------------------------------------------------------ GPU side
@@ -515,7 +561,7 @@ def run_ours(args):
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
         if not strong:
-            line["avg_err_vs_fp64"] = fp64_average_error(job)
+            line["avg_err_vs_fp64"] = precision_check(job)
     print(json.dumps(line))
 
 

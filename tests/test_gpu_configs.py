@@ -1,0 +1,55 @@
+"""Whole-run error curves against the FP64 oracle at the large-instance size.
+
+The large single-instance configuration runs RAAR (beta 0.87) and then DM on
+a 1024^2 pattern (60 ellipses in a 256^2 box, 1e7 photons, Poisson).  Here
+the first 100 RAAR iterations and the 40 DM iterations that follow run on
+the GPU (one engine call each, fixed support) and in FP64 through the oracle
+from the same random-phase start, and the per-iteration modulus error
+E = sum(|F| - M)^2 / sum M^2 is compared iteration by iteration.  Projection
+iterations are chaotic, so the comparison covers the start of the run, where
+FP32 rounding has not yet been amplified; tolerance 1e-3 relative per
+iteration.  The DM part also checks that the error's growth under the
+reference's DM update (phasing.py:1287-1328, phasing_dm1.cl / phasing_dm2.cl)
+is the reference algorithm's own: the FP64 oracle shows the same curve."""
+import numpy as np
+import pytest
+
+from oracle import phasing_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_raar_then_dm_1024_error_curve_vs_fp64():
+    import torch
+    from als_speckle_b200 import synth
+    from als_speckle_b200.engine import Engine, TrialSpec
+    _, M, S = synth.config_pattern("raar_dm_1024", seed=0)
+    N = M.shape[0]
+    assert N == 1024
+    m2 = float(np.sum(M.astype(np.float64) ** 2))
+    Md, Sd = torch.from_numpy(M).cuda(), torch.from_numpy(S).cuda()
+    psi = torch.zeros((N, N), dtype=torch.complex64, device="cuda")
+    e1 = torch.zeros((100, 2), dtype=torch.float64, device="cuda")
+    e2 = torch.zeros((40, 2), dtype=torch.float64, device="cuda")
+    eng = Engine(use_graph=False)
+    eng.solve([TrialSpec(psi=psi, modulus=Md, support=Sd, iterations=100, order=(("raar", 100),),
+                         beta=0.87, random_phase=True, seed=7, trial=0, errors=e1)])
+    eng.solve([TrialSpec(psi=psi, modulus=Md, support=Sd, iterations=40, order=(("dm", 40),),
+                         beta=0.87, errors=e2)])
+    torch.cuda.synchronize()
+    eng.close()
+    gpu = np.concatenate([e1.cpu().numpy()[:, 0], e2.cpu().numpy()[:, 0]]) / m2
+
+    p0 = O.seed_random_phase(M, S, 7, 0, mode="f64")
+    p1, r1 = O.iterate(p0, M, S, 100, order=(("raar", 100),), beta=0.87, mode="f64", errors=True)
+    _, r2 = O.iterate(p1, M, S, 40, order=(("dm", 40),), beta=0.87, mode="f64", errors=True)
+    f64 = np.concatenate([r1[:, 0], r2[:, 0]])
+    rel = np.abs(gpu - f64) / f64
+    for i in list(range(0, 100, 10)) + list(range(100, 140, 5)) + [139]:
+        print("iteration %3d %s: E gpu %.6e fp64 %.6e rel %.1e"
+              % (i + 1, "raar" if i < 100 else "dm", gpu[i], f64[i], rel[i]))
+    print("max relative deviation: raar %.2e, dm %.2e" % (rel[:100].max(), rel[100:].max()))
+    assert rel.max() < 1e-3
+    # the DM stretch follows the oracle's growth, not just its level
+    g, f = np.diff(gpu[100:]), np.diff(f64[100:])
+    assert np.all(np.sign(g) == np.sign(f)) or np.abs(g - f).max() < 1e-3 * np.abs(f).max()

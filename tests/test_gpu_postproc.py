@@ -28,8 +28,8 @@ def unw():
 
 
 def _rel(a, b):
-    return float(np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64)) /
-                 np.linalg.norm(np.asarray(b, np.float64)))
+    a, b = np.asarray(a, np.complex128), np.asarray(b, np.complex128)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def test_unwrap_512_matches_reference(unw):
