@@ -5,7 +5,11 @@ over time.  The service admits them against an HBM budget as earlier
 requests finish, and advances every admitted trial in rounds: one engine call
 per round moves each active trial forward by up to ``chunk`` iterations, so
 requests of different sizes, algorithms and lengths share the same launches
-and new requests join at the next round.  Between rounds a trial's state is
+and new requests join at the next round.  Rounds are pipelined: round k+1 is
+built and enqueued before round k's results are collected, so the device
+always has queued work while the host reads back one batch of per-request
+finiteness flags, copies finished results out on a second stream and admits
+new requests.  Between rounds a trial's state is
 only its psi (the Fourier work plane is rebuilt from psi at the start of a
 round, which is the same arithmetic the uninterrupted iteration performs), so
 a request's result does not depend on what else is in flight.
@@ -106,22 +110,45 @@ class _Active:
                                   device=device)
         algs, counts = expand_runs(req.order)
         self.flat = [a for a, c in zip(algs, counts) for _ in range(c)]
-        self.done = 0
+        self.done = 0        # iterations whose round has completed
+        self.scheduled = 0   # iterations enqueued (one round may be in flight beyond done)
+        self.last_round = -1  # the latest round that uses this request's buffers
+        self.dead = False    # diverged or cancelled while a round held it
         self.admitted = admitted
         self.bytes = req.bytes_needed()
 
     def specs(self, chunk):
-        n = min(chunk, self.req.iterations - self.done)
-        last = self.done + n >= self.req.iterations
-        order = rotated_order(self.flat, self.done)
+        """The next round's trials: up to ``chunk`` iterations from where the
+        enqueued work ends."""
+        start = self.scheduled
+        n = min(chunk, self.req.iterations - start)
+        last = start + n >= self.req.iterations
+        order = rotated_order(self.flat, start)
         out = []
         for k in range(self.req.trials):
             out.append(TrialSpec(
                 psi=self.psi[k], modulus=self.M, support=self.S, iterations=n, order=order,
-                beta=self.req.beta, random_phase=(self.done == 0), seed=self.req.seed, trial=k,
+                beta=self.req.beta, random_phase=(start == 0), seed=self.req.seed, trial=k,
                 box=self.box if last else None, save=self.save[k] if last else None,
-                errors=self.errors[k, self.done:self.done + n], quirks="gpu"))
+                errors=self.errors[k, start:start + n], quirks="gpu"))
         return n, out
+
+
+class _Round:
+    """One enqueued engine call: its requests with their iteration counts,
+    the per-request finiteness flags (pinned host copy) and the event that
+    marks the round's end on the service stream."""
+
+    def __init__(self, index, members, flags_host, event):
+        self.index = index
+        self.members = members  # [(active, n)]
+        self.flags_host = flags_host
+        self.event = event
+
+    def wait(self):
+        if self.event is not None:
+            self.event.synchronize()
+        return [bool(v) for v in self.flags_host.tolist()]
 
 
 class ServingEngine:
@@ -147,7 +174,11 @@ class ServingEngine:
         self.in_use = 0
         self.rounds = 0
         self.trial_iterations = 0
-        self.stream = torch.cuda.Stream(self.device) if self.device.type == "cuda" else None
+        cuda = self.device.type == "cuda"
+        self.stream = torch.cuda.Stream(self.device) if cuda else None
+        self.copy_stream = torch.cuda.Stream(self.device) if cuda else None
+        self._inflight: Optional[_Round] = None
+        self._retiring: List[_Active] = []
 
     def _on_stream(self):
         return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
@@ -165,7 +196,8 @@ class ServingEngine:
 
     def cancel(self, rid: int):
         """Drop a request whether it is waiting or in flight; its result is
-        recorded with status "cancelled" and its memory is released."""
+        recorded with status "cancelled" and its memory is released (once no
+        enqueued round uses it any more)."""
         for i, (_, r, req) in enumerate(self.pending):
             if r == rid:
                 self.pending.pop(i)
@@ -177,12 +209,21 @@ class ServingEngine:
         for a in self.active:
             if a.req.rid == rid:
                 self.active.remove(a)
-                self.in_use -= a.bytes
                 self.results[rid] = Result(rid, np.zeros((0, 0, 0), np.complex64),
                                            np.zeros((0, 0, 2)), a.box, a.req.arrival, a.admitted,
                                            -1.0, "cancelled")
+                self._retire(a)
                 return True
         return False
+
+    def _retire(self, a):
+        """Release a request's memory now, or after the last enqueued round
+        that uses its buffers."""
+        a.dead = True
+        if self._inflight is not None and a.last_round >= self._inflight.index:
+            self._retiring.append(a)
+        else:
+            self.in_use -= a.bytes
 
     def _admit(self, now):
         trials = sum(a.req.trials for a in self.active)
@@ -198,62 +239,111 @@ class ServingEngine:
             self.in_use += a.bytes
             trials += req.trials
 
+    def _enqueue(self, members):
+        """Enqueue one round: the engine call and the per-request finiteness
+        flags of its last iteration (copied to pinned host memory behind it).
+        Returns the round without waiting for it."""
+        specs, used = [], []
+        for a in members:
+            n, sp = a.specs(self.chunk)
+            a.scheduled += n
+            a.last_round = self.rounds
+            specs.extend(sp)
+            used.append((a, n))
+            self.trial_iterations += n * a.req.trials
+        with self._on_stream():
+            self.engine.solve(specs, stream=self.stream)
+            flags = torch.stack([torch.isfinite(a.errors[:, a.scheduled - 1]).all()
+                                 for a, n in used])
+            event = None
+            if self.stream is not None:
+                host = torch.empty(flags.shape, dtype=torch.bool, pin_memory=True)
+                host.copy_(flags, non_blocking=True)
+                event = torch.cuda.Event()
+                event.record(self.stream)
+            else:
+                host = flags
+        r = _Round(self.rounds, used, host, event)
+        self.rounds += 1
+        return r
+
+    def _host_copy(self, t, event):
+        """Copy a result buffer to the host behind ``event`` on the copy stream,
+        so the round enqueued after it keeps running."""
+        if self.copy_stream is None:
+            return t.numpy().copy()
+        with torch.cuda.stream(self.copy_stream):
+            self.copy_stream.wait_event(event)
+            out = t.to("cpu", non_blocking=True)
+        self.copy_stream.synchronize()
+        return out.numpy()
+
+    def _complete(self, r: _Round, t, realtime):
+        """Account for a finished round: requests whose last iteration was in
+        it are done (their crops and error sums are copied out), requests whose
+        error sums turned non-finite are stopped."""
+        finite = r.wait()
+        # trim the graph cache of launch shapes that have come and gone; the
+        # queued round must finish first (one pipeline bubble per trim)
+        if getattr(self.engine, "use_graph", False) and \
+                _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
+            if self.stream is not None:
+                self.stream.synchronize()
+            _lib.call("sp_engine_release_graphs")
+        for a, n in r.members:
+            a.done += n
+            if a.dead:
+                continue
+            status = None
+            if not finite[r.members.index((a, n))]:
+                status = "diverged"  # the iterate has become non-finite
+            elif a.done >= a.req.iterations:
+                status = "done"
+            if status is None:
+                continue
+            self.results[a.req.rid] = Result(
+                a.req.rid, self._host_copy(a.save, r.event), self._host_copy(a.errors, r.event),
+                a.box, a.req.arrival if realtime else 0.0, a.admitted if realtime else 0.0, t,
+                status)
+            self.active.remove(a)
+            self._retire(a)
+        # memory of stopped requests whose last round has now finished
+        keep = []
+        for a in self._retiring:
+            if a.last_round <= r.index:
+                self.in_use -= a.bytes
+            else:
+                keep.append(a)
+        self._retiring = keep
+
     def run(self, clock=None, realtime=True):
         """Serve until every submitted request is finished.  With
         ``realtime`` the arrival times are honoured against ``clock``
         (seconds); otherwise every request is available immediately.
-        Returns the results by request id."""
+
+        Rounds are pipelined: the next round is built and enqueued while the
+        current one runs (which trials finish when is known in advance; only
+        a divergence is learnt afterwards, and costs the diverged request at
+        most one extra round), so the GPU is not left idle while the host
+        collects results and admits requests.  Returns the results by request
+        id."""
         clock = clock or time.perf_counter
         t0 = clock()
         now = lambda: (clock() - t0) if realtime else float("inf")
-        while self.pending or self.active:
+        while self.pending or self.active or self._inflight is not None:
             self._admit(now())
-            if not self.active:
+            ready = [a for a in self.active if not a.dead and a.scheduled < a.req.iterations]
+            nxt = self._enqueue(ready) if ready else None
+            if self._inflight is not None:
+                done, self._inflight = self._inflight, nxt
+                self._complete(done, clock() - t0, realtime)
+            elif nxt is not None:
+                self._inflight = nxt
+            else:
                 # idle until the next arrival
-                wait = self.pending[0][0] - now()
+                wait = self.pending[0][0] - now() if self.pending else 0.0
                 if wait > 0:
                     time.sleep(min(wait, 0.01))
-                continue
-            specs, steps = [], []
-            for a in self.active:
-                n, sp = a.specs(self.chunk)
-                specs.extend(sp)
-                steps.append(n)
-                self.trial_iterations += n * a.req.trials
-            with self._on_stream():
-                self.engine.solve(specs, stream=self.stream)
-                # one device-side finiteness flag per request, read back in a
-                # single copy (the round's only host synchronisation)
-                flags = torch.stack([torch.isfinite(a.errors[:, a.done + n - 1]).all() if n else
-                                     torch.ones((), dtype=torch.bool, device=self.device)
-                                     for a, n in zip(self.active, steps)])
-                finite = flags.cpu().tolist()
-            # the stream is idle here (the flags were read back): a safe point
-            # to drop cached graphs of launch shapes that have come and gone
-            if getattr(self.engine, "use_graph", False) and \
-                    _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
-                _lib.call("sp_engine_release_graphs")
-            self.rounds += 1
-            t = (clock() - t0)
-            still = []
-            for a, n, ok in zip(self.active, steps, finite):
-                a.done += n
-                if n and not ok:
-                    # the iterate has become non-finite: stop it and free its slots
-                    self.results[a.req.rid] = Result(
-                        a.req.rid, a.save.cpu().numpy(), a.errors.cpu().numpy(), a.box,
-                        a.req.arrival if realtime else 0.0, a.admitted if realtime else 0.0, t,
-                        "diverged")
-                    self.in_use -= a.bytes
-                    continue
-                if a.done >= a.req.iterations:
-                    self.results[a.req.rid] = Result(
-                        a.req.rid, a.save.cpu().numpy(), a.errors.cpu().numpy(), a.box,
-                        a.req.arrival if realtime else 0.0, a.admitted if realtime else 0.0, t)
-                    self.in_use -= a.bytes
-                else:
-                    still.append(a)
-            self.active = still
         return self.results
 
 

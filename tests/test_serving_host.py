@@ -135,7 +135,9 @@ def test_diverged_request_is_stopped_and_freed():
     srv.submit(_req(1, N=32, iters=12))
     res = srv.run(realtime=False)
     assert res[1].status == "diverged" and res[0].status == "done"
-    assert len(eng.calls) == 3 and [len(c) for c in eng.calls] == [4, 2, 2]
+    # rounds are pipelined: round 2 was enqueued before round 1's divergence
+    # was read back, so the diverged request rides along once more, then stops
+    assert len(eng.calls) == 3 and [len(c) for c in eng.calls] == [4, 4, 2]
     assert srv.in_use == 0
 
 
@@ -151,3 +153,25 @@ def test_cancel_pending_and_active():
     res = srv.run(realtime=False)
     assert res[0].status == "cancelled" and res[1].status == "cancelled"
     assert eng.calls == []
+
+
+def test_next_round_is_enqueued_before_the_current_one_completes():
+    """Pipelined rounds: when round k is collected, round k+1 is already on
+    the stream (the GPU is never left without queued work while the host
+    collects results and admits requests)."""
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    srv = ServingEngine(device="cpu", chunk=4, engine=eng)
+    seen = []
+    orig = srv._complete
+
+    def spy(r, t, realtime):
+        seen.append((r.index, len(eng.calls)))
+        return orig(r, t, realtime)
+
+    srv._complete = spy
+    srv.submit(_req(0, iters=12))
+    res = srv.run(realtime=False)
+    assert res[0].status == "done" and srv.in_use == 0
+    # rounds 0 and 1 are collected with one more round already enqueued
+    assert seen == [(0, 2), (1, 3), (2, 3)]
