@@ -47,9 +47,13 @@ class phasing(common):
         self.use_gpu = True
         self.compute_device = "gpu"
         self.quirks = quirks
-        self.engine = engine or Engine(device=self.device, use_graph=False)
+        # the engine runs on a private stream ordered after (and before) the
+        # caller's current stream, so its launch sequence can be replayed as a
+        # CUDA graph (graphs cannot be captured on the legacy default stream)
+        self.engine = engine or Engine(device=self.device, use_graph=True)
         with torch.cuda.device(self.device):
             call("sp_device_init")
+            self._stream = torch.cuda.Stream(self.device)
         self.modulus_state = 0
         self.support_state = 0
         self.ipsf_state = 0
@@ -295,11 +299,15 @@ class phasing(common):
         crop into ``savebuffer[numtrial]`` (``phasing.py:181-289``).
 
         The per-iteration FP64 modulus error sums of FFT(psi_in) are kept in
-        ``self.errors`` (see ``modulus_error``)."""
-        if debug_on:
-            raise NotImplementedError("debug_on FITS dumps are not supported")
+        ``self.errors`` (see ``modulus_error``).  Iterations listed in
+        ``debug_on`` run one operator at a time and write the reference's
+        debugging FITS files to the working directory (``_debug_iteration``);
+        the others run fused."""
         self._check_ready()
         iterations = int(iterations)
+        debug = set(int(i) for i in (debug_on or ()))
+        if debug and (self._ipsf() is not None or self._spectrum() is not None):
+            raise NotImplementedError("debug_on dumps cover the coherent projection only")
         if self.numtrial >= self.savebuffer.shape[0]:
             raise IndexError("savebuffer is full (%d slots); load(numtrials=...) to enlarge"
                              % self.savebuffer.shape[0])
@@ -311,23 +319,86 @@ class phasing(common):
         self.errors = torch.zeros((iterations, 2), dtype=torch.float64, device=self.device)
         done = 0
         while done < iterations:
-            n = min(chunk, iterations - done)
-            rot = [flat[(done + i) % len(flat)] for i in range(len(flat))]
-            last = done + n >= iterations
-            spec = TrialSpec(psi=self.psi_in, modulus=self.modulus, support=self.support,
-                             iterations=n, order=_runs_from_flat(rot), beta=beta,
-                             box=(self.r0, self.c0, self.rows, self.cols) if last else None,
-                             save=self.savebuffer[self.numtrial] if last else None,
-                             errors=self.errors[done:done + n], quirks="gpu", ipsf=self._ipsf(),
-                             spectrum=self._spectrum())
-            self.engine.solve([spec])
+            if done in debug:
+                self._debug_iteration(flat[done % len(flat)], done, beta)
+                n = 1
+            else:
+                n = min(chunk, iterations - done)
+                nxt = [i for i in debug if i > done]
+                if nxt:
+                    n = min(n, min(nxt) - done)
+                rot = [flat[(done + i) % len(flat)] for i in range(len(flat))]
+                last = done + n >= iterations
+                spec = TrialSpec(psi=self.psi_in, modulus=self.modulus, support=self.support,
+                                 iterations=n, order=_runs_from_flat(rot), beta=beta,
+                                 box=(self.r0, self.c0, self.rows, self.cols) if last else None,
+                                 save=self.savebuffer[self.numtrial] if last else None,
+                                 errors=self.errors[done:done + n], quirks="gpu",
+                                 ipsf=self._ipsf(), spectrum=self._spectrum())
+                self._solve([spec])
             done += n
             if silent is not True and (isinstance(silent, bool) or done % chunk == 0):
                 print("  iteration %s" % done)
-        if iterations == 0:
+        if iterations == 0 or (iterations - 1) in debug:
             self._kexec("copy_to_buffer_f2", self.savebuffer, self.psi_in, self.c0, self.r0,
                         self.numtrial, self.N, shape=(self.cols, self.rows))
         self.numtrial += 1
+
+    def _debug_iteration(self, alg, iteration, beta):
+        """One iteration through the operator API, as the reference's GPU
+        branch runs it (``phasing.py:1187-1353``: FFT, divisor |FFT|, the
+        ``fourier`` kernel, inverse FFT, then the update kernel; DM repeats the
+        projection on ``dm1(psi_in)``), saving what the reference's debug mode
+        saves (``phasing.py:1193-1227``, ``:1244-1246``) under the same names:
+        ``gpu i<it> psi_fourier_1`` / ``fourier_div`` / ``psi_fourier_2``
+        (fftshifted, magnitude and phase), ``gpu i<it> out`` (real and
+        imaginary) and, for HIO, ``gpu i<it> hio update``.  The iteration's
+        FP64 error sums go to ``self.errors[iteration]`` as the fused path's do."""
+        from . import io
+        shift = np.fft.fftshift
+        tag = "%s i%s " % (self.compute_device, iteration)
+        N = self.N
+        st = stream_ptr()
+        m = self.modulus
+
+        def constraint(data):
+            pf = torch.empty_like(data)
+            call("sp_fft2", ptr(data), ptr(pf), N, 1, 0, st)
+            io.save(tag + "psi_fourier_1.fits", shift(self.get(pf)), components="polar")
+            div = torch.empty_like(pf)
+            self._cl_abs(pf, div)
+            io.save(tag + "fourier_div.fits", shift(self.get(div)), components="polar")
+            self._kexec("fourier", pf, div, m, pf)
+            io.save(tag + "psi_fourier_2.fits", shift(self.get(pf)), components="polar")
+            out = torch.empty_like(pf)
+            call("sp_fft2", ptr(pf), ptr(out), N, 1, 1, st)
+            io.save(tag + "out.fits", self.get(out), components="cartesian")
+            return out, div
+
+        psi, sup = self.psi_in, self.support
+        out, div = constraint(psi)
+        d = div.real.double() - m.double()
+        self.errors[iteration, 0] = (d * d).sum()
+        self.errors[iteration, 1] = d.abs().sum()
+        name = _CODE_NAMES[alg]
+        if name == "hio":
+            self._kexec("hio", beta, sup, psi, out, psi)
+            io.save(tag + "hio update.fits", self.get(psi), components="cartesian")
+        elif name == "er":
+            self._kexec("er", sup, out, psi)
+        elif name == "raar":
+            self._kexec("raar", beta, sup, psi, out, psi)
+        elif name == "sf":
+            self._kexec("sf", sup, psi, out, psi)
+        elif name == "er_cpu":  # phasing.py:1257
+            psi.mul_(sup)
+        elif name == "sf_cpu":  # phasing.py:1284
+            psi.copy_((1 - sup) * (-psi) + sup * out)
+        else:  # dm: gamma_m = 1/beta, gamma_s = -gamma_m (phasing.py:1294-1295)
+            tmp = torch.empty_like(psi)
+            self._kexec("dm1", 1.0 / beta, sup, psi, tmp)
+            tmp, _ = constraint(tmp)
+            self._kexec("dm2", beta, -1.0 / beta, sup, psi, out, tmp, psi)
 
     def iterate_trials(self, iterations, trials, order=None, beta=0.8, seed=0,
                        random_phase=True, errors=False):
@@ -356,9 +427,19 @@ class phasing(common):
                                    save=self.savebuffer[self.numtrial + k],
                                    errors=errs[k] if errors else None, quirks=self.quirks,
                                    ipsf=self._ipsf(), spectrum=self._spectrum()))
-        self.engine.solve(specs)
+        self._solve(specs)
         self.numtrial += trials
         return (psis, errs) if errors else psis
+
+    def _solve(self, specs):
+        """Run the engine on the private stream, ordered after everything the
+        caller's current stream has queued and before anything it queues
+        next."""
+        cur = torch.cuda.current_stream(self.device)
+        self._stream.wait_stream(cur)
+        with torch.cuda.stream(self._stream):
+            self.engine.solve(specs, stream=self._stream)
+        cur.wait_stream(self._stream)
 
     def modulus_error(self):
         """Per-iteration (E, R) of the last ``iterate``: E = sum(|F|-M)^2/sum M^2,
