@@ -42,6 +42,13 @@ __device__ __forceinline__ float2 turn(long long num, long long den) {
   sincospif(2.0f * (float)((double)r / (double)den), &s, &c);
   return make_float2(c, s);
 }
+// the same for a power-of-two denominator N: the residue is a mask (two's
+// complement gives the non-negative residue of a negative numerator too)
+__device__ __forceinline__ float2 turn_pow2(int num, int N) {
+  float s, c;
+  sincospif(2.0f * (float)(num & (N - 1)) / (float)N, &s, &c);
+  return make_float2(c, s);
+}
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(kRegThreads) reg_upsample_rows_kernel(
       if (ky < N && kx < N) {
         const long long idx = (long long)ky * N + kx;
         v = cmulc(Ff[idx], R[idx]);
-        v = cmul(v, turn((long long)signed_freq(ky, N) * d0.x + (long long)signed_freq(kx, N) * d0.y, N));
+        v = cmul(v, turn_pow2(signed_freq(ky, N) * d0.x + signed_freq(kx, N) * d0.y, N));
       }
       xs[rr * (kRegK + 1) + kk] = v;
     }
@@ -232,44 +239,60 @@ __global__ void __launch_bounds__(kRegThreads) reg_upsample_cols_kernel(
   if ((threadIdx.x & 31) == 0) atomicMax(&best_up[f], mine);
 }
 
-// Per frame: the refined shift d = d0 + (p* - h, q* - h)/U (as the integer
-// numerators d U), the phase of c at the peak (recomputed in FP64 from T1),
-// and the result record shifts[f] = (dy, dx, theta).
+// Per frame (one warp each): the refined shift d = d0 + (p* - h, q* - h)/U
+// (as the integer numerators d U), the phase of c at the peak (recomputed in
+// FP64 from T1), and the result record shifts[f] = (dy, dx, theta).
 __global__ void reg_finish_kernel(const float2* __restrict__ T1, const float2* __restrict__ W,
                                   const unsigned long long* __restrict__ best,
                                   const unsigned long long* __restrict__ best_up, int n, int N,
                                   int U, int M, int2* __restrict__ num, double* __restrict__ shifts) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
   if (f >= n) return;
   const int2 d0 = coarse_shift(best[f], N);
   const uint32_t idx = 0xffffffffu - (uint32_t)(best_up[f] & 0xffffffffu);
   const int p = (int)(idx / M), q = (int)(idx % M), h = M / 2;
   const float2* t1 = T1 + (long long)f * N * M;
   double re = 0.0, im = 0.0;
-  for (int ky = 0; ky < N; ++ky) {
+  for (int ky = lane; ky < N; ky += 32) {
     const float2 w = W[(long long)ky * M + p], t = t1[(long long)ky * M + q];
     re += (double)w.x * t.x - (double)w.y * t.y;
     im += (double)w.x * t.y + (double)w.y * t.x;
   }
-  const int ny = d0.x * U + (p - h), nx = d0.y * U + (q - h);
-  num[f] = make_int2(ny, nx);
-  shifts[3 * f] = (double)ny / U;
-  shifts[3 * f + 1] = (double)nx / U;
-  shifts[3 * f + 2] = atan2(im, re);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  if (lane == 0) {
+    const int ny = d0.x * U + (p - h), nx = d0.y * U + (q - h);
+    num[f] = make_int2(ny, nx);
+    shifts[3 * f] = (double)ny / U;
+    shifts[3 * f + 1] = (double)nx / U;
+    shifts[3 * f + 2] = atan2(im, re);
+  }
 }
 
-// F_f <- F_f exp(2 pi i k.d/N) exp(-i theta), d = num / U
-__global__ void reg_shift_kernel(float2* __restrict__ F, int n, int N, int U,
-                                 const int2* __restrict__ num, const double* __restrict__ shifts) {
+// F_f <- F_f exp(2 pi i k.d/N) exp(-i theta), d = num / U.  With
+// num = d0 U + (p - h) per axis the ramp factors into the whole-pixel turn
+// exp(2 pi i k d0 / N) and the kernel-table entry W[k][p] = exp(2 pi i k (p - h)/(U N)).
+__global__ void reg_shift_kernel(float2* __restrict__ F, int n, int N, int U, int M,
+                                 const float2* __restrict__ W, const int2* __restrict__ num,
+                                 const double* __restrict__ shifts) {
   const long long NN = (long long)N * N, total = (long long)n * NN;
+  const int h = M / 2;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
        k += (long long)gridDim.x * blockDim.x) {
     const int f = (int)(k / NN);
     const long long rem = k - f * NN;
     const int ky = (int)(rem / N), kx = (int)(rem - (long long)ky * N);
     const int2 d = num[f];
-    const float2 w = turn((long long)signed_freq(ky, N) * d.x + (long long)signed_freq(kx, N) * d.y,
-                          (long long)U * N);
+    // floor division of the numerators by U: d = d0 U + (p - h), p - h in [-h, h]
+    const int d0y = (d.x + h) >= 0 ? (d.x + h) / U : -((-(d.x + h) + U - 1) / U);
+    const int d0x = (d.y + h) >= 0 ? (d.y + h) / U : -((-(d.y + h) + U - 1) / U);
+    const int py = d.x - d0y * U + h, px = d.y - d0x * U + h;
+    float2 w = turn_pow2(signed_freq(ky, N) * d0y + signed_freq(kx, N) * d0x, N);
+    w = cmul(w, cmul(W[(long long)ky * M + py], W[(long long)kx * M + px]));
     const double th = shifts[3 * f + 2];
     F[k] = cmul(F[k], cmul(w, make_float2((float)cos(th), (float)-sin(th))));
   }
@@ -367,11 +390,11 @@ extern "C" int sp_register_subpixel(const void* frames_dev, int n_frames, int ro
   reg_upsample_rows_kernel<<<dim3((N + kRegRows - 1) / kRegRows, n_frames), kRegThreads, smem, st>>>(
       F, Rf, W, best, X, N, M);
   reg_upsample_cols_kernel<<<dim3((M + 7) / 8, n_frames), kRegThreads, 0, st>>>(X, W, N, M, best_up);
-  reg_finish_kernel<<<(n_frames + 127) / 128, 128, 0, st>>>(X, W, best, best_up, n_frames, N, U, M,
-                                                            num, shifts_dev);
+  reg_finish_kernel<<<(n_frames + 3) / 4, 128, 0, st>>>(X, W, best, best_up, n_frames, N, U, M,
+                                                        num, shifts_dev);
   SP_CUDA_TRY(cudaGetLastError());
   if (out_dev) {
-    reg_shift_kernel<<<grid(n_frames * NN), 256, 0, st>>>(F, n_frames, N, U, num, shifts_dev);
+    reg_shift_kernel<<<grid(n_frames * NN), 256, 0, st>>>(F, n_frames, N, U, M, W, num, shifts_dev);
     SP_CUDA_TRY(cudaGetLastError());
     SP_CUDA_TRY(fft2_dispatch(F, F, N, n_frames, 1, st));  // inverse, scaled by 1/N^2
     reg_crop_kernel<<<grid((long long)n_frames * rows * cols), 256, 0, st>>>(F, (float2*)out_dev,

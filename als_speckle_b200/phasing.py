@@ -53,7 +53,7 @@ class phasing(common):
         self.engine = engine or Engine(device=self.device, use_graph=True)
         with torch.cuda.device(self.device):
             call("sp_device_init")
-            self._stream = torch.cuda.Stream(self.device)
+            self._engine_stream = torch.cuda.Stream(self.device)
         self.modulus_state = 0
         self.support_state = 0
         self.ipsf_state = 0
@@ -361,18 +361,22 @@ class phasing(common):
         st = stream_ptr()
         m = self.modulus
 
+        def dump(name, array, components):
+            # DM projects twice per iteration under the same names: keep the last
+            io.save(tag + name + ".fits", array, components=components, overwrite=True)
+
         def constraint(data):
             pf = torch.empty_like(data)
             call("sp_fft2", ptr(data), ptr(pf), N, 1, 0, st)
-            io.save(tag + "psi_fourier_1.fits", shift(self.get(pf)), components="polar")
+            dump("psi_fourier_1", shift(self.get(pf)), "polar")
             div = torch.empty_like(pf)
             self._cl_abs(pf, div)
-            io.save(tag + "fourier_div.fits", shift(self.get(div)), components="polar")
+            dump("fourier_div", shift(self.get(div)), "polar")
             self._kexec("fourier", pf, div, m, pf)
-            io.save(tag + "psi_fourier_2.fits", shift(self.get(pf)), components="polar")
+            dump("psi_fourier_2", shift(self.get(pf)), "polar")
             out = torch.empty_like(pf)
             call("sp_fft2", ptr(pf), ptr(out), N, 1, 1, st)
-            io.save(tag + "out.fits", self.get(out), components="cartesian")
+            dump("out", self.get(out), "cartesian")
             return out, div
 
         psi, sup = self.psi_in, self.support
@@ -383,7 +387,7 @@ class phasing(common):
         name = _CODE_NAMES[alg]
         if name == "hio":
             self._kexec("hio", beta, sup, psi, out, psi)
-            io.save(tag + "hio update.fits", self.get(psi), components="cartesian")
+            dump("hio update", self.get(psi), "cartesian")
         elif name == "er":
             self._kexec("er", sup, out, psi)
         elif name == "raar":
@@ -436,10 +440,10 @@ class phasing(common):
         caller's current stream has queued and before anything it queues
         next."""
         cur = torch.cuda.current_stream(self.device)
-        self._stream.wait_stream(cur)
-        with torch.cuda.stream(self._stream):
-            self.engine.solve(specs, stream=self._stream)
-        cur.wait_stream(self._stream)
+        self._engine_stream.wait_stream(cur)
+        with torch.cuda.stream(self._engine_stream):
+            self.engine.solve(specs, stream=self._engine_stream)
+        cur.wait_stream(self._engine_stream)
 
     def modulus_error(self):
         """Per-iteration (E, R) of the last ``iterate``: E = sum(|F|-M)^2/sum M^2,
