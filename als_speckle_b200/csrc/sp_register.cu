@@ -120,20 +120,24 @@ __global__ void reg_kernel_table(float2* __restrict__ W, int N, int U, int M) {
 
 // T1[f][ky][q] = sum_kx X_f'[ky][kx] W[kx][q], X_f' = F_f conj(R) exp(2 pi i k.d0/N).
 // CTA: 32 rows ky of one frame, all M columns; kx in chunks of 32 through
-// shared memory; thread = (row group of 4, column group of M/... ) register tile.
+// shared memory.  The modulation is separable, exp(2 pi i ky d0y/N) times
+// exp(2 pi i kx d0x/N): the CTA's row factors are made once, each chunk's
+// column factors once per chunk.  Thread (tr, tq) accumulates the register
+// tile of rows tr + 8 j (j < 4) and columns tq + 32 m (m < 8, up to M).
 constexpr int kRegRows = 32, kRegK = 32, kRegThreads = 256;
 __global__ void __launch_bounds__(kRegThreads) reg_upsample_rows_kernel(
     const float2* __restrict__ F, const float2* __restrict__ R, const float2* __restrict__ W,
     const unsigned long long* __restrict__ best, float2* __restrict__ T1, int N, int M) {
   extern __shared__ float2 sm[];
-  float2* xs = sm;                       // [kRegRows][kRegK + 1]
+  float2* xs = sm;                           // [kRegRows][kRegK + 1]
   float2* ws = sm + kRegRows * (kRegK + 1);  // [kRegK][M]
+  __shared__ float2 rowf[kRegRows], colf[kRegK];
   const int f = blockIdx.y;
   const int ky0 = blockIdx.x * kRegRows;
   const long long NN = (long long)N * N;
   const int2 d0 = coarse_shift(best[f], N);
   const float2* Ff = F + f * NN;
-  // thread tile: rows r0 + 8 j (j < 4), columns q0 + 32 m (m < ceil(M/32))
+  if (threadIdx.x < kRegRows) rowf[threadIdx.x] = turn_pow2(signed_freq(ky0 + threadIdx.x, N) * d0.x, N);
   const int tr = threadIdx.x / 32, tq = threadIdx.x % 32;
   constexpr int MQ = 8;  // up to 256 columns
   float2 acc[4][MQ];
@@ -142,6 +146,8 @@ __global__ void __launch_bounds__(kRegThreads) reg_upsample_rows_kernel(
 #pragma unroll
     for (int m = 0; m < MQ; ++m) acc[j][m] = make_float2(0.f, 0.f);
   for (int kx0 = 0; kx0 < N; kx0 += kRegK) {
+    __syncthreads();  // the previous chunk's tiles are consumed
+    if (threadIdx.x < kRegK) colf[threadIdx.x] = turn_pow2(signed_freq(kx0 + threadIdx.x, N) * d0.y, N);
     __syncthreads();
     for (int i = threadIdx.x; i < kRegRows * kRegK; i += blockDim.x) {
       const int rr = i / kRegK, kk = i - rr * kRegK;
@@ -149,8 +155,7 @@ __global__ void __launch_bounds__(kRegThreads) reg_upsample_rows_kernel(
       float2 v = make_float2(0.f, 0.f);
       if (ky < N && kx < N) {
         const long long idx = (long long)ky * N + kx;
-        v = cmulc(Ff[idx], R[idx]);
-        v = cmul(v, turn_pow2(signed_freq(ky, N) * d0.x + signed_freq(kx, N) * d0.y, N));
+        v = cmul(cmul(cmulc(Ff[idx], R[idx]), rowf[rr]), colf[kk]);
       }
       xs[rr * (kRegK + 1) + kk] = v;
     }

@@ -175,10 +175,20 @@ class Engine:
             self._ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
         return self._ws
 
+    # cached CUDA graphs (one per workspace and launch shape, process-wide)
+    # kept before solve drops them all
+    MAX_GRAPHS = 64
+
     def solve(self, trials: Sequence[TrialSpec], stream=None):
         """Enqueue every trial's iterations on ``stream`` (asynchronous)."""
         if not trials:
             return
+        if self.use_graph and _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
+            # a long-lived caller whose launch shapes keep changing (different
+            # iteration counts, trial mixes): drop the cache once nothing runs
+            for d in range(torch.cuda.device_count()):
+                torch.cuda.synchronize(d)
+            call("sp_engine_release_graphs")
         arr = (_lib.sp_trial * len(trials))(*[_to_struct(t) for t in trials])
         need = C.c_size_t(0)
         call("sp_engine_workspace_size", arr, len(trials), C.byref(need))
