@@ -46,6 +46,11 @@ cudaError_t twiddles(const float2** out);
 
 inline cudaStream_t as_stream(sp_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// The fused engine (sp_engine.cu); `concurrent` allows the per-size launch
+// chains to run on forked auxiliary streams.
+int engine_run(const sp_trial* trials, int n_trials, void* workspace_dev, size_t workspace_bytes,
+               const sp_run_opts* opts, sp_stream_t stream, bool concurrent);
+
 constexpr int kMaxN = 4096;
 constexpr int kMinN = 8;
 constexpr int kThreads = 256;  // every engine/FFT CTA

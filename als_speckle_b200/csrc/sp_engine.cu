@@ -308,6 +308,7 @@ struct Segment {
   int pc_egrid;                     // grid of the tiled rescale kernel
   int col_ticks;                    // the column pass runs at ticks [0, col_ticks)
   int pc_mask;                      // partial-coherence kernels launched (bit = which)
+  int ticks;                        // ticks of this segment's longest trial (n_iter + 1)
 };
 
 struct GraphKey {
@@ -323,29 +324,96 @@ static std::mutex g_graph_mutex;
 static std::map<GraphKey, cudaGraphExec_t> g_graphs;
 static thread_local int64_t g_last_launches = 0;
 
-static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, const Item* items,
-                        const int2* jobs, int n_ticks, const float2* tw, cudaStream_t st) {
-  for (int k = 0; k < n_ticks; ++k) {
+// One segment's launch chain: per tick its partial-coherence kernels, its
+// column pass and its row pass.
+static int launch_segment(const Segment& sg, const Slot* slots, const Item* items,
+                          const int2* jobs, const float2* tw, cudaStream_t st) {
+  for (int k = 0; k < sg.ticks; ++k) {
     // partially coherent projections first (their slots sit out the column pass)
-    for (const Segment& sg : segs) {
-      if (sg.pc_count == 0) continue;
+    if (sg.pc_count > 0) {
       PcArgs pa{slots, jobs + sg.pc_first, sg.pc_count, k, tw};
       for (int which = 0; which < 5; ++which)
         if (sg.pc_mask & (1 << which))
           SP_CUDA_TRY(launch_pc(sg.N, which, which == 3 ? sg.pc_egrid : sg.pc_grid, st, pa));
     }
     for (int which = 0; which < 2; ++which) {
-      for (const Segment& sg : segs) {
-        if (which == 0 && k >= sg.col_ticks) continue;  // no column work left in this segment
-        // the column pass walks the items backwards: it starts on the
-        // trials whose G planes the row pass wrote last (still in L2), and
-        // the next row pass starts on the ones it wrote last
-        PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw, which == 0 ? 1 : 0};
-        SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid[which], st, a));
-      }
+      if (which == 0 && k >= sg.col_ticks) continue;  // no column work left in this segment
+      // the column pass walks the items backwards: it starts on the trials
+      // whose G planes the row pass wrote last (still in L2), and the next
+      // row pass starts on the ones it wrote last
+      PassArgs a{slots, items + sg.first, sg.count, nullptr, k, tw, which == 0 ? 1 : 0};
+      SP_CUDA_TRY(launch_pass(sg.N, sg.E, which, sg.grid[which], st, a));
     }
   }
   return SP_OK;
+}
+
+// Auxiliary streams and events of the calling thread, per device, for the
+// concurrent segment chains (created before any capture begins).
+struct ForkPool {
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;  // [0] fork, [1 + i] join of stream i
+};
+static thread_local std::map<int, ForkPool> t_fork;
+
+static cudaError_t fork_pool(int dev, int branches, ForkPool** out) {
+  ForkPool& P = t_fork[dev];
+  while ((int)P.streams.size() < branches) {
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    P.streams.push_back(s);
+  }
+  while ((int)P.events.size() < branches + 1) {
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    P.events.push_back(ev);
+  }
+  *out = &P;
+  return cudaSuccess;
+}
+
+// Every segment of a group, each as its own chain: segments share no data
+// (their trials, planes and items are disjoint; slots, items and transposed
+// moduli are only read), so the chains of different sizes run concurrently
+// -- the first on `st`, the others on auxiliary streams forked from it and
+// joined back into it (in a capture this forms parallel graph branches).  The
+// joins are made even after a failed launch, so a capture never ends with
+// unjoined work.
+static int launch_ticks(const std::vector<Segment>& segs, const Slot* slots, const Item* items,
+                        const int2* jobs, const float2* tw, ForkPool* P, cudaStream_t st) {
+  if (segs.size() == 1 || P == nullptr) {
+    for (const Segment& sg : segs) {
+      const int rc = launch_segment(sg, slots, items, jobs, tw, st);
+      if (rc != SP_OK) return rc;
+    }
+    return SP_OK;
+  }
+  const int n_aux = (int)segs.size() - 1;
+  SP_CUDA_TRY(cudaEventRecord(P->events[0], st));
+  int rc = SP_OK;
+  int forked = 0;
+  for (int i = 0; i < n_aux; ++i) {
+    if (cudaStreamWaitEvent(P->streams[i], P->events[0], 0) != cudaSuccess) {
+      set_error("cudaStreamWaitEvent failed while forking segment %d", i + 1);
+      rc = SP_ERR_CUDA;
+      break;
+    }
+    forked = i + 1;
+    if (rc == SP_OK) rc = launch_segment(segs[i + 1], slots, items, jobs, tw, P->streams[i]);
+  }
+  if (rc == SP_OK) rc = launch_segment(segs[0], slots, items, jobs, tw, st);
+  for (int i = 0; i < forked; ++i) {
+    const cudaError_t e1 = cudaEventRecord(P->events[1 + i], P->streams[i]);
+    const cudaError_t e2 = cudaStreamWaitEvent(st, P->events[1 + i], 0);
+    if (rc == SP_OK && (e1 != cudaSuccess || e2 != cudaSuccess)) {
+      set_error("joining segment %d failed: %s", i + 1,
+                cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+      rc = SP_ERR_CUDA;
+    }
+  }
+  return rc;
 }
 
 }  // namespace sp
@@ -363,8 +431,11 @@ extern "C" int sp_engine_workspace_size(const sp_trial* trials, int n_trials, si
   return SP_OK;
 }
 
-extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspace_dev,
-                             size_t workspace_bytes, const sp_run_opts* opts, sp_stream_t stream) {
+// sp_engine_run's body; `concurrent` lets the chains of different sizes run
+// on forked auxiliary streams (sp_engine_run_static keeps them on `stream`:
+// it creates no streams or events).
+int sp::engine_run(const sp_trial* trials, int n_trials, void* workspace_dev, size_t workspace_bytes,
+                   const sp_run_opts* opts, sp_stream_t stream, bool concurrent) {
   SP_CHECK(n_trials >= 0, SP_ERR_INVALID, "n_trials < 0");
   if (n_trials == 0) return SP_OK;
   SP_CHECK(trials != nullptr, SP_ERR_INVALID, "trials is null");
@@ -419,7 +490,9 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
       if (count == 0) continue;
       int occ[2] = {1, 1}, sms = 1;
       SP_CUDA_TRY(occupancy_for(N, E, occ, &sms));
-      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1, 1, 0, 0};
+      Segment sg{N, E, first, count, {1, 1}, (int)hj.size(), 0, 1, 1, 0, 0, 0};
+      for (int i = gstart[g]; i < gstart[g + 1]; ++i)
+        if (trials[i].n == N) sg.ticks = std::max(sg.ticks, trials[i].n_iter + 1);
       // Partially coherent slots project in their own kernels: the column
       // pass has work for them only at tick 0, to start a random phase.  A
       // segment of such slots alone launches it only while it has work.
@@ -524,16 +597,21 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
   const int2* djobs = reinterpret_cast<const int2*>(ws + L.jobs_off);
   const bool use_graph = opts && opts->use_graph && st != nullptr;
   g_last_launches = (int64_t)L.mt_first.size();
+  size_t max_segs = 1;
   for (int g = 0; g < n_groups; ++g) {
+    max_segs = std::max(max_segs, segs[g].size());
     for (const Segment& sg : segs[g]) {
-      g_last_launches += ticks[g] + std::min(ticks[g], sg.col_ticks);
-      g_last_launches += (int64_t)__builtin_popcount(sg.pc_mask) * ticks[g];
+      g_last_launches += sg.ticks + std::min(sg.ticks, sg.col_ticks);
+      g_last_launches += (int64_t)__builtin_popcount(sg.pc_mask) * sg.ticks;
     }
   }
+  // auxiliary streams for concurrent segment chains, made before any capture
+  ForkPool* pool = nullptr;
+  if (concurrent && max_segs > 1) SP_CUDA_TRY(fork_pool(dev, (int)max_segs - 1, &pool));
 
   for (int g = 0; g < n_groups; ++g) {
     if (!use_graph) {
-      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, ticks[g], tw, st);
+      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, tw, pool, st);
       if (rc != SP_OK) return rc;
       continue;
     }
@@ -541,7 +619,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     for (const Segment& sg : segs[g])
       key.shape.insert(key.shape.end(), {sg.N, sg.E, sg.first, sg.count, sg.grid[0], sg.grid[1],
                                          sg.pc_first, sg.pc_count, sg.pc_grid, sg.pc_egrid,
-                                         std::min(ticks[g], sg.col_ticks), sg.pc_mask});
+                                         std::min(sg.ticks, sg.col_ticks), sg.pc_mask, sg.ticks});
     cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);
@@ -551,7 +629,7 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     if (!exec) {
       cudaGraph_t graph = nullptr;
       SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, ticks[g], tw, st);
+      const int rc = launch_ticks(segs[g], dslots, ditems, djobs, tw, pool, st);
       const cudaError_t ce = cudaStreamEndCapture(st, &graph);
       if (rc != SP_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -567,6 +645,11 @@ extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspa
     SP_CUDA_TRY(cudaGraphLaunch(exec, st));
   }
   return SP_OK;
+}
+
+extern "C" int sp_engine_run(const sp_trial* trials, int n_trials, void* workspace_dev,
+                             size_t workspace_bytes, const sp_run_opts* opts, sp_stream_t stream) {
+  return engine_run(trials, n_trials, workspace_dev, workspace_bytes, opts, stream, true);
 }
 
 extern "C" int64_t sp_engine_last_launches(void) { return g_last_launches; }

@@ -63,5 +63,7 @@ extern "C" int sp_engine_run_static(const sp_trial* trials, int n_trials, const 
   // Nothing in the scratch needs to start at zero: the descriptor tables are
   // written by sp_engine_run on every call and each work plane is written
   // before it is read.
-  return sp_engine_run(trials, n_trials, scratch, kStaticScratchBytes, &o, stream);
+  // The launch chains of different sizes stay on the caller's stream here
+  // (concurrent chains would create auxiliary streams and events).
+  return engine_run(trials, n_trials, scratch, kStaticScratchBytes, &o, stream, false);
 }
