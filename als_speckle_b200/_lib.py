@@ -74,6 +74,7 @@ _SIGS = {
     "sp_engine_release_graphs": ([], _i),
     "sp_engine_last_launches": ([], C.c_int64),
     "sp_engine_graph_count": ([], C.c_int64),
+    "sp_engine_release_device_graphs": ([], _i),
     "sp_engine_run_static": ([C.POINTER(sp_trial), _i, C.POINTER(sp_run_opts), _p], _i),
     "sp_hio": ([_f, _p, _p, _p, _p, _i64, _p], _i),
     "sp_er": ([_p, _p, _p, _i64, _p], _i),

@@ -659,6 +659,21 @@ extern "C" int64_t sp_engine_graph_count(void) {
   return (int64_t)g_graphs.size();
 }
 
+extern "C" int sp_engine_release_device_graphs(void) {
+  int dev = 0;
+  SP_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  for (auto it = g_graphs.begin(); it != g_graphs.end();) {
+    if (it->first.dev == dev) {
+      cudaGraphExecDestroy(it->second);
+      it = g_graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return SP_OK;
+}
+
 extern "C" int sp_engine_release_graphs(void) {
   std::lock_guard<std::mutex> lock(g_graph_mutex);
   for (auto& kv : g_graphs) cudaGraphExecDestroy(kv.second);

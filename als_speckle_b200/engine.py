@@ -185,10 +185,11 @@ class Engine:
             return
         if self.use_graph and _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
             # a long-lived caller whose launch shapes keep changing (different
-            # iteration counts, trial mixes): drop the cache once nothing runs
-            for d in range(torch.cuda.device_count()):
-                torch.cuda.synchronize(d)
-            call("sp_engine_release_graphs")
+            # iteration counts, trial mixes): drop this device's cached graphs
+            # once nothing runs on it
+            torch.cuda.synchronize(self.device)
+            with torch.cuda.device(self.device):
+                call("sp_engine_release_device_graphs")
         arr = (_lib.sp_trial * len(trials))(*[_to_struct(t) for t in trials])
         need = C.c_size_t(0)
         call("sp_engine_workspace_size", arr, len(trials), C.byref(need))

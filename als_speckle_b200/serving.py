@@ -287,9 +287,9 @@ class ServingEngine:
         # queued round must finish first (one pipeline bubble per trim)
         if getattr(self.engine, "use_graph", False) and \
                 _lib.lib.sp_engine_graph_count() > self.MAX_GRAPHS:
-            if self.stream is not None:
-                self.stream.synchronize()
-            _lib.call("sp_engine_release_graphs")
+            torch.cuda.synchronize(self.device)
+            with torch.cuda.device(self.device):
+                _lib.call("sp_engine_release_device_graphs")
         for a, n in r.members:
             a.done += n
             if a.dead:

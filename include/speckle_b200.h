@@ -119,6 +119,9 @@ int sp_engine_release_graphs(void);
  * and launch shape); a long-running caller whose shapes keep changing can
  * release them (sp_engine_release_graphs) once its stream is idle. */
 int64_t sp_engine_graph_count(void);
+/* Destroy only the cached graphs of the calling thread's current device
+ * (none of them may be running: synchronise that device first). */
+int sp_engine_release_device_graphs(void);
 /* Kernel launches enqueued by the calling thread's last sp_engine_run
  * (kernels inside a launched graph count individually). */
 int64_t sp_engine_last_launches(void);
