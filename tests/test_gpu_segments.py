@@ -54,3 +54,27 @@ def test_concurrent_size_chains_equal_alone_and_count_launches():
         # and a row pass, the 64^2 chain sized by its longer (7-iteration) trial
         assert int(_lib.lib.sp_engine_last_launches()) == 4 + 2 * (8 + 10 + 4)
         eng.close()
+
+
+def test_graph_cache_is_trimmed_and_results_hold():
+    """An engine whose launch shapes keep changing (here: iteration counts)
+    drops its device's cached graphs once it holds more than MAX_GRAPHS, and
+    every solve still gives the eager result."""
+    from als_speckle_b200 import _lib
+    from als_speckle_b200.engine import Engine
+    M, S, _, _ = _inputs()[1]
+    stream = torch.cuda.Stream()
+    eager = Engine(use_graph=False, e_per_n={})
+    graphed = Engine(use_graph=True, e_per_n={})
+    graphed.MAX_GRAPHS = 2
+    for iters in (2, 3, 4, 5, 6):
+        a = torch.zeros(M.shape, dtype=torch.complex64, device="cuda")
+        b = torch.zeros(M.shape, dtype=torch.complex64, device="cuda")
+        with torch.cuda.stream(stream):
+            eager.solve(_specs([a], [(M, S, iters, "hio")]), stream=stream)
+            graphed.solve(_specs([b], [(M, S, iters, "hio")]), stream=stream)
+        stream.synchronize()
+        assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+        assert int(_lib.lib.sp_engine_graph_count()) <= 3
+    eager.close()
+    graphed.close()
