@@ -559,7 +559,7 @@ def run_ours(args):
     }
     if serving is not None:
         line["serving"] = serving
-    if args.cpu_baseline:
+    if args.cpu_baseline and world == 1:  # the host-core baseline: rank 0 at N = 1 only
         line["cpu_baseline"] = cpu_baseline()
         if not strong:
             line["avg_err_vs_fp64"] = precision_check(job)
