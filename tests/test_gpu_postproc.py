@@ -100,3 +100,22 @@ def test_prtf_512_32_frames_vs_oracle():
     assert np.max(np.abs(arr.cpu().numpy() - want)) < 2e-5
     want_q = O.unwrap_average(arr.cpu().numpy())
     assert np.allclose(q.cpu().numpy(), want_q, rtol=1e-5, atol=1e-6)
+
+
+def test_unwrap_general_grid_vs_oracle():
+    """sp_unwrap on an inner radius, an off-centre centre and an explicit
+    column count against the oracle's restatement of wrapping.unwrap (which
+    makes scipy's map_coordinates call)."""
+    import torch
+    from als_speckle_b200._lib import call, ptr, stream_ptr
+    m = golden_inputs.smooth_map(128, 5)
+    r_in, r_out, cy, cx, cols = 5, 40, 60.0, 70.0, 150
+    a = torch.from_numpy(m).cuda()
+    work = torch.empty((128, 128), dtype=torch.float64, device="cuda")
+    uw = torch.empty((r_out - r_in, cols), dtype=torch.float32, device="cuda")
+    mean = torch.empty(r_out - r_in, dtype=torch.float32, device="cuda")
+    call("sp_unwrap", ptr(a), 128, r_in, r_out, cy, cx, cols, ptr(work), ptr(uw), ptr(mean),
+         stream_ptr())
+    want = O.unwrap(m, r_in, r_out, (cy, cx), columns=cols)
+    assert np.allclose(uw.cpu().numpy(), want, rtol=1e-5, atol=1e-6)
+    assert np.allclose(mean.cpu().numpy(), want.mean(axis=1), rtol=1e-5, atol=1e-6)

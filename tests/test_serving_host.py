@@ -175,3 +175,33 @@ def test_next_round_is_enqueued_before_the_current_one_completes():
     assert res[0].status == "done" and srv.in_use == 0
     # rounds 0 and 1 are collected with one more round already enqueued
     assert seen == [(0, 2), (1, 3), (2, 3)]
+
+
+def test_cancel_while_a_round_is_queued_defers_the_release():
+    """Cancelling a request that the queued round still uses: its result is
+    "cancelled" at once, its memory is released only after that round, and it
+    takes part in no round after it."""
+    from als_speckle_b200.serving import ServingEngine
+    eng = FakeEngine()
+    srv = ServingEngine(device="cpu", chunk=4, engine=eng)
+    srv.submit(_req(0, N=16, iters=16))
+    srv.submit(_req(1, N=32, iters=16))
+    orig = srv._complete
+    seen = []
+
+    def spy(r, t, realtime):
+        out = orig(r, t, realtime)
+        if r.index == 0:
+            before = srv.in_use
+            assert srv.cancel(1)
+            # round 1 (already queued) still holds request 1's buffers
+            seen.append((before, srv.in_use))
+        return out
+
+    srv._complete = spy
+    res = srv.run(realtime=False)
+    assert res[1].status == "cancelled" and res[0].status == "done"
+    assert seen[0][0] == seen[0][1]  # nothing released while round 1 is queued
+    assert srv.in_use == 0
+    # request 1 (N = 32) is in rounds 0 and 1 only
+    assert [sum(1 for c in call if c[0] == 32) for call in eng.calls] == [2, 2, 0, 0]
