@@ -290,12 +290,12 @@ class ServingEngine:
             torch.cuda.synchronize(self.device)
             with torch.cuda.device(self.device):
                 _lib.call("sp_engine_release_device_graphs")
-        for a, n in r.members:
+        for (a, n), ok in zip(r.members, finite):
             a.done += n
             if a.dead:
                 continue
             status = None
-            if not finite[r.members.index((a, n))]:
+            if not ok:
                 status = "diverged"  # the iterate has become non-finite
             elif a.done >= a.req.iterations:
                 status = "done"
