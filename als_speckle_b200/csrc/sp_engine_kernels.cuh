@@ -463,13 +463,23 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
         cp_async_wait_all();
         sync();
         if (active) {
+          // two copies of the loop, so that no element carries a select
+          // between psi and zero (ER and SF never read psi)
+          if (cf.needs_pi) {
 #pragma unroll
-          for (int i = 0; i < E; ++i) {
-            const float sv = sup_s[i * T];
-            const float wa = cf.a0 + cf.a1 * sv;
-            const float wb = cf.b0 + cf.b1 * sv;
-            const float2 pi = cf.needs_pi ? psi_s[i * T] : make_float2(0.f, 0.f);
-            v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa - v[i].y * wb);
+            for (int i = 0; i < E; ++i) {
+              const float sv = sup_s[i * T];
+              const float wa = cf.a0 + cf.a1 * sv;
+              const float wb = cf.b0 + cf.b1 * sv;
+              const float2 pi = psi_s[i * T];
+              v[i] = make_float2(pi.x * wa + v[i].x * wb, pi.y * wa - v[i].y * wb);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+              const float wb = cf.b0 + cf.b1 * sup_s[i * T];
+              v[i] = make_float2(v[i].x * wb, -v[i].y * wb);
+            }
           }
           // DM: the update without -s*b*t waits in the psi tile
           if (nf == 2) {
