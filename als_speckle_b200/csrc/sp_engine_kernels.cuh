@@ -168,19 +168,28 @@ __device__ __forceinline__ void cp_async_rows(void* sdst, const void* gsrc, int 
   constexpr int CHUNKS = ROWS * PER_ROW;
   char* d = static_cast<char*>(sdst);
   const char* g = static_cast<const char*>(gsrc);
+  if constexpr (PER_ROW % NT == 0) {
+    // thread q0 (< NT) copies chunks q0 + j*NT: row j / (PER_ROW/NT), chunk
+    // q0 + (j % (PER_ROW/NT))*NT of that row -- one per-thread base plus
+    // compile-time offsets, no index arithmetic per copy
+    constexpr int PER = PER_ROW / NT;
+    d += q0 * 16;
+    g += q0 * 16;
 #pragma unroll
-  for (int j = 0; j < (CHUNKS + NT - 1) / NT; ++j) {
-    const int q = q0 + j * NT;
-    if (CHUNKS % NT == 0 || q < CHUNKS) {
-      const int r = q / PER_ROW, c = q - r * PER_ROW;  // PER_ROW is a power of two
+    for (int j = 0; j < CHUNKS / NT; ++j) {
+      const int r = j / PER, c = (j % PER) * NT;
       cp_async<16>(d + r * SP + c * 16, g + (size_t)r * GP + c * 16);
     }
+  } else {
+#pragma unroll
+    for (int j = 0; j < (CHUNKS + NT - 1) / NT; ++j) {
+      const int q = q0 + j * NT;
+      if (CHUNKS % NT == 0 || q < CHUNKS) {
+        const int r = q / PER_ROW, c = q - r * PER_ROW;  // PER_ROW is a power of two
+        cp_async<16>(d + r * SP + c * 16, g + (size_t)r * GP + c * 16);
+      }
+    }
   }
-}
-// the same, shared by the whole block
-template <int ROWS, int RB, int GP, int SP>
-__device__ __forceinline__ void cp_async_tile(void* sdst, const void* gsrc) {
-  cp_async_rows<ROWS, RB, GP, SP, kThreads>(sdst, gsrc, threadIdx.x);
 }
 
 // Shared-memory plan of one pass item.  Row pass: exchange strips | twiddles |
@@ -601,13 +610,15 @@ __device__ __forceinline__ void copy_col_plane(const float2* plane, int block, f
   using CS = ColSmem<N, E, TH>;
   using BF = ColButterflies<N, E, TH>;
   const BF bf;
-  const float2* g = plane + block * CS::C + bf.c;
+  // this thread's first row of the tile; every copy is that base plus a
+  // compile-time offset of whole rows
+  const float2* g = plane + block * CS::C + bf.c + (size_t)bf.j0 * N;
 #pragma unroll
   for (int u = 0; u < BF::U; ++u) {
     if (bf.valid(u)) {
 #pragma unroll
       for (int r = 0; r < CS::RL; ++r)
-        cp_async<8>(gbuf + bf.pa(u, r), g + (size_t)(bf.j(u) + r * CS::NSL) * N);
+        cp_async<8>(gbuf + bf.pa(u, r), g + (size_t)(u * BF::JS + r * CS::NSL) * N);
     }
   }
 }
@@ -643,16 +654,17 @@ __device__ __forceinline__ void col_last_stage(float2* g, int block, const float
     }
   }
   then();
-  float2* dst = g + block * CS::C + bf.c;
+  // per-thread bases; the butterflies' rows and twiddles are compile-time offsets from them
+  float2* dst = g + block * CS::C + bf.c + (size_t)bf.j0 * N;
+  const float2* __restrict__ twj = tws + bf.j0;
 #pragma unroll
   for (int u = 0; u < BF::U; ++u) {
     if (bf.valid(u)) {
-      const int j = bf.j(u);
 #pragma unroll
-      for (int r = 1; r < R; ++r) x[u][r] = cmul(x[u][r], tws[r * NS + j]);
+      for (int r = 1; r < R; ++r) x[u][r] = cmul(x[u][r], twj[r * NS + u * BF::JS]);
       dft<R, -1>(x[u]);
 #pragma unroll
-      for (int r = 0; r < R; ++r) dst[(size_t)(j + r * NS) * N] = x[u][r];
+      for (int r = 0; r < R; ++r) dst[(size_t)(u * BF::JS + r * NS) * N] = x[u][r];
     }
   }
 }
@@ -671,12 +683,25 @@ __device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick,
   constexpr int CHUNKS = CS::CG * PER_COL;
   const float* src = s.modulus_t + (size_t)(block * CS::C + lc0) * N;
   float* dst = mod + lc0 * CS::MP;
+  if constexpr (PER_COL % CS::GT == 0) {
+    // chunk gtid + k*GT is column k / (PER_COL/GT), offset gtid + (k % (PER_COL/GT))*GT:
+    // a per-thread base plus compile-time offsets
+    constexpr int PER = PER_COL / CS::GT;
+    src += gtid * 4;
+    dst += gtid * 4;
 #pragma unroll
-  for (int k = 0; k < (CHUNKS + CS::GT - 1) / CS::GT; ++k) {
-    const int q = gtid + k * CS::GT;
-    if (CHUNKS % CS::GT == 0 || q < CHUNKS) {
-      const int cc = q / PER_COL, off = (q - cc * PER_COL) * 4;
+    for (int k = 0; k < CHUNKS / CS::GT; ++k) {
+      const int cc = k / PER, off = (k % PER) * CS::GT * 4;
       cp_async<16>(dst + cc * CS::MP + off, src + (size_t)cc * N + off);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < (CHUNKS + CS::GT - 1) / CS::GT; ++k) {
+      const int q = gtid + k * CS::GT;
+      if (CHUNKS % CS::GT == 0 || q < CHUNKS) {
+        const int cc = q / PER_COL, off = (q - cc * PER_COL) * 4;
+        cp_async<16>(dst + cc * CS::MP + off, src + (size_t)cc * N + off);
+      }
     }
   }
 }
