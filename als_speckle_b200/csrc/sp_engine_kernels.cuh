@@ -549,14 +549,20 @@ __device__ __forceinline__ void project_cols(float2 (&v)[E], const float* m_s, i
 #pragma unroll
   for (int i = 0; i < E; ++i) {
     m[i] = m_s[i * mstride];
-    const float p2 = v[i].x * v[i].x + v[i].y * v[i].y;
-    const float rs = p2 > 0.f ? rsqrtf(p2) : 0.f;
-    const float d = p2 * rs - m[i];  // |F| - M (|F| = 0 gives -M)
+    // The reference divides by |F| = 0 (phasing_fourier.cl:14); here F = 0
+    // keeps M with zero phase, without a select: 2^-62 added to the real part
+    // turns F = 0 into (2^-62, 0), whose |F|^2 = 2^-124 is still a normal
+    // float, so the projection below gives (M/N^2, -0) through power-of-two
+    // scalings and |F| - M = -M.  Real parts of magnitude >= 2^-37 do not
+    // change (the addend is below half their ulp).
+    const float x = v[i].x + 0x1p-62f;
+    const float p2 = x * x + v[i].y * v[i].y;
+    const float rs = rsqrtf(p2);
+    const float d = p2 * rs - m[i];  // |F| - M
     f2 = fmaf(d, d, f2);
     f1 += fabsf(d);
-    // the reference divides by |F| = 0 (phasing_fourier.cl:14); keep M, zero phase
     const float sc = m[i] * rs * inv;
-    v[i] = p2 > 0.f ? make_float2(v[i].x * sc, v[i].y * -sc) : make_float2(m[i] * inv, 0.f);
+    v[i] = make_float2(x * sc, v[i].y * -sc);
   }
   if (want_err) {
     e2 += (double)f2;

@@ -551,6 +551,9 @@ def run_ours(args):
                                              "sp::col_pass_kernel<512,%d>" % tune["E"], min(tune["E"], 32),
                                              group),
                      "traffic": traffic_per_tick(group)},
+        # 10 N^2 log2(N^2) flop per forward + inverse 2-D FFT pair, one pair per
+        # trial-iteration, over the same tick
+        "fft_tflops": 10.0 * N * N * math.log2(N * N) * group / per_tick / 1e12,
         "plain_gpu": plain,
         "single_trial_engine": single,
         "batched_over_plain": value / world / plain["value"],
