@@ -5,7 +5,7 @@ before the library exists.
 """
 import importlib
 
-__all__ = ["phasing", "engine", "masking", "synth", "serving", "distributed", "workloads"]
+__all__ = ["phasing", "engine", "masking", "io", "gpu", "synth", "serving", "distributed", "workloads"]
 
 
 def __getattr__(name):

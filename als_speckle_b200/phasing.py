@@ -12,10 +12,13 @@ Differences from the reference, all deliberate:
   reference's CPU-branch forms instead (``phasing.py:1257``, ``:1284``).
 * Where ``|FFT(psi)| == 0`` the reference divides by zero
   (``phasing_fourier.cl:14``); here the modulus is kept with zero phase.
-* ``debug_on`` FITS dumps are not supported and raise.  ``ipsf`` (transverse
-  coherence) and ``spectrum`` (longitudinal coherence, the reference's
-  GPU-only ``radial_rescale``) are supported; where the blurred divisor is 0
-  the modulus is kept with zero phase, like the coherent case.
+* ``debug_on`` FITS dumps cover the coherent projection (they raise with an
+  ipsf or a spectrum loaded).  ``ipsf`` (transverse coherence) and
+  ``spectrum`` (longitudinal coherence, the reference's GPU-only
+  ``radial_rescale``) are supported; where the blurred divisor is 0 the
+  modulus is kept with zero phase, like the coherent case.
+* ``reconstruct`` runs what the reference's version describes (that one
+  cannot run as written), all trials of a round in one engine call.
 """
 from __future__ import annotations
 
@@ -435,6 +438,73 @@ class phasing(common):
         self.numtrial += trials
         return (psis, errs) if errors else psis
 
+    def reconstruct(self, iterations=100, rounds=1, order=None, refine_support=True,
+                    refinement_parameters=None):
+        """Seed and iterate every trial, average them, refine the support;
+        ``rounds`` times (``phasing.py:932-988``).
+
+        The reference's method cannot run as written (it loops over the
+        integer ``rounds`` and reads an undefined ``self.trials``); this runs
+        what it describes.  Per round, each of the ``numtrials`` trials is
+        seeded as ``seed()`` seeds (numpy's global RNG, in trial order) and
+        iterated ``iterations`` times with ``order`` (default
+        ``(('hio', 99), ('er', 1))``) at beta 0.8 into the next savebuffer
+        slot, all trials in one engine call (the same arithmetic as one
+        ``iterate`` per trial); ``psi_in`` is left holding the last trial's
+        iterate.  A copy of the savebuffer is aligned by each frame's global
+        phase and its last slot is replaced by the mean over all slots, that
+        slot included, as the reference's ``np.mean(save_buffer, axis=0)``
+        is; the mean is ``self.reconstruction`` (numpy).  With
+        ``refine_support`` the support's crop is refined from the mean
+        (``refine_support`` with ``local_threshold`` 0.08, ``blur_sigma`` 3,
+        ``global_threshold`` 0.0 unless ``refinement_parameters`` overrides
+        them; ``kill_weakest`` is accepted and, as in the reference, not
+        used), placed at the corner of an N x N plane and loaded, which
+        restarts the trial count.  A refinement that leaves no pixel raises
+        ValueError (the reference would load a support of NaNs)."""
+        if refinement_parameters is not None and not isinstance(refinement_parameters, dict):
+            raise TypeError("refinement_parameters must be a dict or None")
+        rp = {"local_threshold": 0.08, "blur_sigma": 3, "global_threshold": 0.0,
+              "kill_weakest": False}
+        if refinement_parameters is not None:
+            rp.update(refinement_parameters)
+        beta = 0.8
+        for _ in range(int(rounds)):
+            self._check_ready()
+            T = int(self.numtrials)
+            if self.numtrial + T > self.savebuffer.shape[0]:
+                raise IndexError("savebuffer has %d free slots, %d trials requested"
+                                 % (self.savebuffer.shape[0] - self.numtrial, T))
+            starts = np.empty((T, self.N, self.N), np.complex64)
+            for k in range(T):
+                s = (np.random.rand(self.N, self.N) + 1j * np.random.rand(self.N, self.N))
+                starts[k] = s.astype(np.complex64) * self._support_host
+            psis = torch.from_numpy(starts).to(self.device)
+            algs, counts = expand_runs(order, self.quirks)
+            runs = _runs_from_flat([a for a, c in zip(algs, counts) for _ in range(c)])
+            specs = [TrialSpec(psi=psis[k], modulus=self.modulus, support=self.support,
+                               iterations=int(iterations), order=runs, beta=beta,
+                               box=(self.r0, self.c0, self.rows, self.cols),
+                               save=self.savebuffer[self.numtrial + k], quirks="gpu",
+                               ipsf=self._ipsf(), spectrum=self._spectrum()) for k in range(T)]
+            self._solve(specs)
+            self.psi_in.copy_(psis[T - 1])
+            self.numtrial += T
+            frames = align_global_phase(self.savebuffer)
+            frames[-1] = mean_frames(frames)
+            self.reconstruction = frames[-1].cpu().numpy()
+            if refine_support:
+                crop = self._support_host[self.r0:self.r0 + self.rows, self.c0:self.c0 + self.cols]
+                refined = _shrinkwrap(
+                    crop, self.reconstruction, blur=rp["blur_sigma"],
+                    local_threshold=rp["local_threshold"],
+                    global_threshold=rp["global_threshold"])[0]
+                if not np.any(refined > 0):
+                    raise ValueError("the refined support is empty")
+                new_support = np.zeros(self.shape, np.float32)
+                new_support[:refined.shape[0], :refined.shape[1]] = refined
+                self.load(support=new_support)
+
     def _solve(self, specs):
         """Run the engine on the private stream, ordered after everything the
         caller's current stream has queued and before anything it queues
@@ -600,6 +670,11 @@ def refine_support(support, average_mag, blur=3, local_threshold=.2, global_thre
          ptr(work), ptr(blurred), ptr(refined), ptr(sums), stream_ptr())
     ref = refined.cpu().numpy().astype(support.dtype if support.dtype.kind == "f" else np.int64)
     return ref, blurred.cpu().numpy()
+
+
+# the module function under a second name, for methods whose keyword
+# argument ``refine_support`` (a flag, as in the reference) hides it
+_shrinkwrap = refine_support
 
 
 def align_frames_device(frames, align_to, use_mag_only=False):

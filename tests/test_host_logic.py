@@ -94,3 +94,21 @@ def test_tuned_e_table(tmp_path):
     table = autotune.tuned_e_per_n(device_name="NVIDIA B200")
     assert set(table) >= {256, 512, 1024, 2048}
     assert all(e in (8, 16, 32) for e in table.values())
+
+
+def test_package_exposes_the_modules_example_scripts_use():
+    """``import als_speckle_b200 as speckle`` then ``speckle.io.open``,
+    ``speckle.phasing.phasing``, ``speckle.phasing.refine_support`` and
+    ``speckle.masking.bounding_box``, as the reference's phasing examples
+    call them (``examples/basic_phasing_example.py``,
+    ``examples/advanced_phasing_example.py``)."""
+    import als_speckle_b200 as speckle
+    assert callable(speckle.io.open) and callable(speckle.io.save)
+    assert callable(speckle.masking.bounding_box)
+    for name in ("phasing", "refine_support", "align_global_phase", "prtf", "rftf",
+                 "center_of_mass_average", "covar_results", "gpu_prtf", "gpu_rftf"):
+        assert callable(getattr(speckle.phasing, name)), name
+    for name in ("load", "seed", "iterate", "reconstruct", "optimize_coherence", "status", "get"):
+        assert callable(getattr(speckle.phasing.phasing, name)), name
+    with pytest.raises(AttributeError):
+        speckle.no_such_module
