@@ -220,13 +220,18 @@ def cpu_cores():
 
 
 def cpu_baseline(iters=24):
+    """The host-core baseline: one trial per core at once (the line's value),
+    and one process alone (numpy's FFT is single-threaded)."""
     pool = CpuPool()
     try:
         value, wall, _ = pool.run(iters)
+        alone = pool.pool.apply(_cpu_task, ((0, iters),))
     finally:
         pool.close()
     return {"value": value, "unit": UNIT, "cores": pool.procs, "kind": pool.kind,
-            "sample": pool.describe(iters) + ", %.1f s wall" % wall}
+            "sample": pool.describe(iters) + ", %.1f s wall" % wall,
+            "single_process": {"value": iters / alone, "unit": UNIT, "cores": 1,
+                               "sample": "1 trial x %d HIO iterations at 512^2, alone" % iters}}
 
 
 def _precision_worker(args):
