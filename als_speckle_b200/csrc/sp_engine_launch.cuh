@@ -190,9 +190,11 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
 
 // Single-buffered column pass: CTAs of kColSbThreads threads, each walking
 // half items (C/2 columns; sub-item j is half j & 1 of item j >> 1), with one
-// G buffer, so three CTAs (12 warps) fit an SM where the pipelined form fits
-// one of 8 warps.  A CTA does not overlap its next tile's copy with its own
-// work; the other CTAs on the SM cover it.  Per half item: wait for the tile,
+// G buffer (55 KB), so several CTAs share an SM where the pipelined form fits
+// one.  Two per SM (8 warps, up to 255 registers) run fastest: three at 170
+// registers and four at 128 give up per-warp parallelism in registers for
+// warps that do not make up for it.  A CTA does not overlap its next tile's
+// copy with its own work; the other CTA on the SM covers it.  Per half item: wait for the tile,
 // barrier, forward transform, projection and inverse transform up to its
 // last stage (col_item), barrier, then the last stage in the row mapping
 // straight to global memory, requesting the next half's modulus and tile
@@ -207,7 +209,7 @@ __host__ __device__ constexpr int col_split(int N, int E) {
 }
 
 template <int N, int E>
-__global__ void __launch_bounds__(kColSbThreads, 3) col_pass_sb_kernel(PassArgs a) {
+__global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs a) {
   constexpr int TH = kColSbThreads;
   constexpr int SPLIT = col_split(N, E);
   using CS = ColSmem<N, E, TH, 1>;
