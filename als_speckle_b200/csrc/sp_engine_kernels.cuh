@@ -635,6 +635,36 @@ __device__ __forceinline__ void copy_col_g(const Slot& s, int block, int tick, f
   if (col_projects(s, tick)) copy_col_plane<N, E, TH>(s.g, block, gbuf);
 }
 
+// Row-major staging buffer for the G tile of the single-buffered column pass:
+// row a of the item's C columns at a * kPitch (C + 2 entries: 80-byte rows,
+// so the 16-byte copies and the first stage's reads, rows t + i*T of two
+// columns per warp, use every bank pair no more than the minimum twice).
+template <int N, int E, int TH>
+struct ColTile {
+  using CS = ColSmem<N, E, TH, 1>;
+  static constexpr int kPitch = CS::C + 2;
+  static constexpr int kOff = (CS::kTotal + 1) & ~1;  // float2 offset, 16-byte aligned
+  static constexpr int kTotal = kOff + N * kPitch;
+};
+
+// Request a plane's tile of a column item into the staging buffer, 16 bytes
+// per cp.async: thread q copies chunks q + j*TH (row (q + j*TH) / Q, chunk
+// q % Q of the row's Q = C/2), so each warp covers whole 32-byte sectors of
+// consecutive rows.  Every thread of the block takes part, and the caller
+// makes sure the whole block has read the buffer's previous tile.
+template <int N, int E, int TH>
+__device__ __forceinline__ void copy_col_tile(const float2* plane, int block, float2* tile) {
+  using CT = ColTile<N, E, TH>;
+  constexpr int C = CT::CS::C, Q = C / 2, ROWS_PER = TH / Q;
+  static_assert(C % 2 == 0 && TH % Q == 0 && N % ROWS_PER == 0, "16-byte chunks of the tile rows");
+  const int q = threadIdx.x;
+  const float2* src = plane + (size_t)block * C + 2 * (q % Q) + (size_t)(q / Q) * N;
+  float2* dst = tile + (q / Q) * CT::kPitch + 2 * (q % Q);
+#pragma unroll
+  for (int j = 0; j < N / ROWS_PER; ++j)
+    cp_async<16>(dst + j * ROWS_PER * CT::kPitch, src + (size_t)j * ROWS_PER * N);
+}
+
 // The last stage of the inverse column transforms of an item whose earlier
 // stages left their (conjugated) outputs in gbuf, run in the row mapping as a
 // forward stage.  Its result, the conjugate of the new work plane, is
@@ -719,15 +749,19 @@ __device__ __forceinline__ void copy_col_mod(const Slot& s, int block, int tick,
 // to its last stage.  Returns the plane that col_last_stage must complete
 // (for DM the first plane is finished here and the second plane's tile
 // brought into the strips, which its transforms need).
-template <int N, int E, int TH = kThreads>
+// With STAGED (the single-buffered pass), the first plane's G tile is read
+// from the row-major staging buffer `tile` instead of the strips.
+template <int N, int E, int TH = kThreads, bool STAGED = false>
 __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, float2* gbuf,
-                                            const float* mod, const float2* __restrict__ tw) {
+                                            const float* mod, const float2* __restrict__ tw,
+                                            const float2* tile = nullptr) {
   using CS = ColSmem<N, E, TH>;
   constexpr int T = CS::T;
   constexpr int C = CS::C;
   constexpr int SH = CS::SH, P = 1 << SH;
   constexpr float inv = 1.0f / ((float)N * (float)N);
   constexpr bool kFull = (C * T == TH);
+  static_assert(!STAGED || kFull, "the staged tile is read by every thread");
   using Sync = typename std::conditional<(T <= 32), WarpSync, LineSync<T>>::type;
   const int tid = threadIdx.x;
   const int lcol = tid / T;
@@ -773,7 +807,17 @@ __device__ __forceinline__ float2* col_item(const Slot& s, int step, int block, 
         }
       }
     }
-    if (active) {  // the plane's tile (or the start values), in the column's strip
+    bool staged = false;
+    if constexpr (STAGED) {
+      if (plane == 0 && step > 0) {  // the tile in the row-major staging buffer
+        constexpr int TP = ColTile<N, E, TH>::kPitch;
+        const float2* tp = tile + t * TP + lc;
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = tp[i * T * TP];
+        staged = true;
+      }
+    }
+    if (!staged && active) {  // the plane's tile (or the start values), in the column's strip
       if constexpr (T % P == 0) {
         const int p0 = padk(t, SH);
 #pragma unroll

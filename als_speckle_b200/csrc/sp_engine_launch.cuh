@@ -190,17 +190,20 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
 
 // Single-buffered column pass: CTAs of kColSbThreads threads, each walking
 // half items (C/2 columns; sub-item j is half j & 1 of item j >> 1), with one
-// G buffer (55 KB), so several CTAs share an SM where the pipelined form fits
-// one.  Two per SM (8 warps, up to 255 registers) run fastest: three at 170
-// registers and four at 128 give up per-warp parallelism in registers for
-// warps that do not make up for it.  A CTA does not overlap its next tile's
-// copy with its own work; the other CTA on the SM covers it.  Per half item: wait for the tile,
-// barrier, forward transform, projection and inverse transform up to its
-// last stage (col_item), barrier, then the last stage in the row mapping
-// straight to global memory, requesting the next half's modulus and tile
-// into the same buffer as its inputs are consumed (each thread overwrites
-// only entries it has read).  Used where it measures faster (512^2 at E = 32;
-// at 1024^2 and above its narrower tiles lose more than the extra warps gain).
+// set of column strips (exchanges and the last stage's inputs) and one
+// row-major staging buffer for the G tile (96 KB in all), so two CTAs share
+// an SM where the pipelined form fits one.  Two per SM (8 warps, up to 255
+// registers) run fastest: with the strips alone (55 KB), three per SM at 170
+// registers and four at 128 were slower, giving up per-warp parallelism in
+// registers for warps that do not make up for it.
+// Per half item: wait for the tile and modulus, barrier, forward transform
+// (its first stage reading the staging buffer), projection and inverse
+// transform up to its last stage (col_item), barrier, then the last stage in
+// the row mapping straight to global memory while the next half's modulus
+// (into the strips it has finished with) and tile (into the staging buffer,
+// 16-byte copies of whole row segments) are requested; the other CTA on the
+// SM covers the copies.  Used where it measures faster (512^2 at E = 32; at
+// 1024^2 and above its narrower tiles lose more than the extra warps gain).
 constexpr int kColSbThreads = 128;
 __host__ __device__ constexpr bool col_single_buffered(int N, int E) { return N == 512 && E == 32; }
 // column-pass work units per item
@@ -219,6 +222,7 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
   const float2* tw = stage_twiddles<N, E>(smem + CS::kTw, a.tw);  // block barrier
   float* mod = reinterpret_cast<float*>(smem + CS::kMod);
+  float2* tile = smem + ColTile<N, E, TH>::kOff;
   const int n_sub = SPLIT * a.n_items;
   int it = blockIdx.x;
   if (it >= n_sub) return;  // the whole block leaves together
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
   __syncthreads();
   copy_col_mod<N, E, TH>(sl[0], i0.block, tick, mod);
   asm volatile("cp.async.commit_group;" ::: "memory");
-  copy_col_g<N, E, TH>(sl[0], i0.block, tick, smem);
+  if (col_projects(sl[0], tick)) copy_col_tile<N, E, TH>(sl[0].g, i0.block, tile);
   asm volatile("cp.async.commit_group;" ::: "memory");
   for (int k = 0; it < n_sub; it += G, ++k) {
     const Item i3 = sub_at(it + 3 * G);
@@ -244,12 +248,14 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
     __syncthreads();      // ... visible to all; the previous sub-item is finished
     const Slot& s = sl[k % 3];
     float2* pend = nullptr;
-    if (col_live(s, tick)) pend = col_item<N, E, TH>(s, tick - s.start_tick, i0.block, smem, mod, tw);
-    __syncthreads();  // last-stage inputs in the strips; the modulus strips consumed
+    if (col_live(s, tick))
+      pend = col_item<N, E, TH, true>(s, tick - s.start_tick, i0.block, smem, mod, tw, tile);
+    __syncthreads();  // last-stage inputs in the strips; the modulus strips and the tile consumed
     auto copies = [&]() {
       if (i1.slot >= 0) copy_col_mod<N, E, TH>(sl[(k + 1) % 3], i1.block, tick, mod);
       asm volatile("cp.async.commit_group;" ::: "memory");
-      if (i1.slot >= 0) copy_col_g<N, E, TH>(sl[(k + 1) % 3], i1.block, tick, smem);
+      if (i1.slot >= 0 && col_projects(sl[(k + 1) % 3], tick))
+        copy_col_tile<N, E, TH>(sl[(k + 1) % 3].g, i1.block, tile);
       if (i2.slot >= 0) copy_slot(&sl[(k + 2) % 3], &a.slots[i2.slot]);  // sub-item k-1's entry
       asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -267,7 +273,7 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
 template <int N, int E>
 constexpr size_t col_smem_bytes() {
   if constexpr (col_single_buffered(N, E))
-    return (size_t)ColSmem<N, E, kColSbThreads, 1>::kTotal * sizeof(float2);
+    return (size_t)ColTile<N, E, kColSbThreads>::kTotal * sizeof(float2);
   else
     return (size_t)ColSmem<N, E>::kTotal * sizeof(float2);
 }
