@@ -349,15 +349,27 @@ static int launch_segment(const Segment& sg, const Slot* slots, const Item* item
 }
 
 // Auxiliary streams and events of the calling thread, per device, for the
-// concurrent segment chains (created before any capture begins).
+// concurrent segment chains (created before any capture begins), released
+// when the thread exits (errors ignored: at process exit the runtime may
+// already be shutting down).
 struct ForkPool {
+  int dev = -1;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;  // [0] fork, [1 + i] join of stream i
+  ForkPool() = default;
+  ForkPool(const ForkPool&) = delete;
+  ForkPool& operator=(const ForkPool&) = delete;
+  ~ForkPool() {
+    if (dev < 0 || (streams.empty() && events.empty()) || cudaSetDevice(dev) != cudaSuccess) return;
+    for (cudaStream_t s : streams) cudaStreamDestroy(s);
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
 };
 static thread_local std::map<int, ForkPool> t_fork;
 
 static cudaError_t fork_pool(int dev, int branches, ForkPool** out) {
   ForkPool& P = t_fork[dev];
+  P.dev = dev;
   while ((int)P.streams.size() < branches) {
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);

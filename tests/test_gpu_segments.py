@@ -78,3 +78,40 @@ def test_graph_cache_is_trimmed_and_results_hold():
         assert int(_lib.lib.sp_engine_graph_count()) <= 3
     eager.close()
     graphed.close()
+
+
+def test_chains_from_threads_that_exit():
+    """Concurrent chains launched from short-lived host threads (each makes
+    its own auxiliary streams, released when it exits) give the same bits as
+    from the main thread."""
+    import threading
+    from als_speckle_b200.engine import Engine
+    inp = _inputs()
+
+    def run(out):
+        psis = [torch.zeros(M.shape, dtype=torch.complex64, device="cuda") for M, _, _, _ in inp]
+        stream = torch.cuda.Stream()
+        eng = Engine(use_graph=False, e_per_n={})
+        with torch.cuda.stream(stream):
+            eng.solve(_specs(psis, inp), stream=stream)
+        stream.synchronize()
+        eng.close()
+        out.extend(p.cpu().numpy() for p in psis)
+
+    want = []
+    run(want)
+    for _ in range(3):
+        got, errors = [], []
+
+        def worker():
+            try:
+                run(got)
+            except Exception as e:  # reported below, on the main thread
+                errors.append(e)
+
+        t = threading.Thread(target=worker)
+        t.start()
+        t.join()
+        assert not errors, errors
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
