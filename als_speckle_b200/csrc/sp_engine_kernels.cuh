@@ -507,8 +507,13 @@ __device__ __forceinline__ bool row_item(const Slot& s, int step, int block, flo
       }
       if (plane == nf - 1) {
         if (active) {
+          // psi is read again only by the next step's update, and ER and SF
+          // (GPU forms) do not read it: before one of those (not at the
+          // run's last step) the store is skipped
+          if (!start || update_coef(alg_s, b).needs_pi) {
 #pragma unroll
-          for (int i = 0; i < E; ++i) psi[i * T] = v[i];
+            for (int i = 0; i < E; ++i) psi[i * T] = v[i];
+          }
           if (!start && s.save != nullptr && row >= s.r0 && row < s.r0 + s.rows) {
             float2* dst = s.save + (size_t)(row - s.r0) * s.cols - s.c0;
 #pragma unroll
