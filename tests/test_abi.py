@@ -77,3 +77,31 @@ def test_host_side_errors_without_gpu(lib):
     assert _lib.lib.sp_engine_run(t, 1, None, 0, None, None) == 1
     with pytest.raises(_lib.SpeckleError):
         _lib.call("sp_fft2", None, None, 512, 1, 0, None)
+
+
+def test_registration_and_unwrap_argument_checks_without_gpu(lib):
+    """The subpixel registration and the polar unwrap reject bad arguments
+    before any CUDA call; the registration workspace size is host
+    arithmetic and grows with the frame count."""
+    from als_speckle_b200 import _lib
+    L = _lib.lib
+    b = C.c_size_t(0)
+    assert L.sp_register_workspace_size(4, 256, 64, C.byref(b)) == 0 and b.value > 0
+    b4 = b.value
+    assert L.sp_register_workspace_size(8, 256, 64, C.byref(b)) == 0 and b.value > b4
+    assert L.sp_register_workspace_size(4, 100, 64, C.byref(b)) == 2   # N not a power of two
+    assert L.sp_register_workspace_size(4, 256, 0, C.byref(b)) == 1    # upsample below 1
+    assert L.sp_register_workspace_size(4, 256, 171, C.byref(b)) == 1  # upsample above 170
+    assert L.sp_register_workspace_size(0, 256, 64, C.byref(b)) == 1   # no frames
+    p = C.c_void_p(256)
+    d = C.cast(p, C.POINTER(C.c_double))
+    # frames larger than N, then a missing reference
+    assert L.sp_register_subpixel(p, 2, 300, 300, p, 256, 64, p, b4, d, p, None) == 1
+    assert L.sp_register_subpixel(p, 2, 100, 100, None, 256, 64, p, b4, d, p, None) == 1
+    f = C.cast(p, C.POINTER(C.c_float))
+    w = C.cast(p, C.POINTER(C.c_double))
+    # no input, no output, empty radius range, grid outside the map
+    assert L.sp_unwrap(None, 64, 0, 32, 32.0, 32.0, 0, w, f, f, None) == 1
+    assert L.sp_unwrap(f, 64, 0, 32, 32.0, 32.0, 0, w, None, None, None) == 1
+    assert L.sp_unwrap(f, 64, 10, 10, 32.0, 32.0, 0, w, f, f, None) == 1
+    assert L.sp_unwrap(f, 64, 0, 40, 32.0, 32.0, 0, w, f, f, None) == 1
