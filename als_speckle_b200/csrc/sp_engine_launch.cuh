@@ -16,6 +16,20 @@ struct PassArgs {
   int reverse;  // walk the item list from its end
 };
 
+// Programmatic dependent launch: a pass kernel lets the next kernel of its
+// stream be scheduled as soon as all of its own CTAs run, and that kernel
+// builds its twiddle tables and reads its descriptors (nothing an earlier
+// kernel writes) while this one finishes, then waits for it to complete
+// before touching any plane.  The wait is the hardware's grid dependency: it
+// ends when the earlier grid has completed and its writes are visible.
+__device__ __forceinline__ void pdl_allow_next() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait_prev() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+
 // Copy one slot descriptor into shared memory (word by word).
 __device__ __forceinline__ void load_slot(Slot* dst, const Slot* __restrict__ src) {
   static_assert(sizeof(Slot) % 4 == 0, "slot size");
@@ -74,6 +88,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_ke
   using RG = RowGroup<N, E>;
   extern __shared__ float2 smem[];
   __shared__ __align__(16) Slot sl[3][RG::NG];
+  pdl_allow_next();
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
   const float2* tw = stage_twiddles<N, E>(smem + SM::kTw, a.tw);  // block barrier
   float* sup_tile = reinterpret_cast<float*>(smem + SM::kSup);
@@ -87,6 +102,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, true)) row_pass_ke
   load_slot_by<RG::GT>(&sl[0][g], &a.slots[i0.slot], gtid);
   if (i1.slot >= 0) load_slot_by<RG::GT>(&sl[1][g], &a.slots[i1.slot], gtid);
   sync();
+  pdl_wait_prev();  // the planes are the previous pass's output
   bool ready = false;
   if (row_finishes(sl[0][g], tick)) {
     prefetch_row_tile<N, E>(sl[0][g], i0.block, smem, g, gtid);
@@ -141,6 +157,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
   using CS = ColSmem<N, E>;
   extern __shared__ float2 smem[];
   __shared__ __align__(16) Slot sl[3];
+  pdl_allow_next();
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
   const float2* tw = stage_twiddles<N, E>(smem + CS::kTw, a.tw);  // block barrier
   float* mod = reinterpret_cast<float*>(smem + CS::kMod);
@@ -152,6 +169,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks_for(E, false)) col_pass_k
   load_slot(&sl[0], &a.slots[i0.slot]);
   if (i1.slot >= 0) load_slot(&sl[1], &a.slots[i1.slot]);
   __syncthreads();
+  pdl_wait_prev();  // the planes (and the transposed modulus) are earlier kernels' output
   copy_col_g<N, E>(sl[0], i0.block, tick, smem);
   asm volatile("cp.async.commit_group;" ::: "memory");
   float2* pend = nullptr;  // plane whose last stage is left in the other buffer
@@ -219,6 +237,7 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
   static_assert(SPLIT * CS::C == lines_per_item(N, E), "an item is SPLIT whole sub-items");
   extern __shared__ float2 smem[];
   __shared__ __align__(16) Slot sl[3];
+  pdl_allow_next();
   const int tick = (a.tick_base ? *a.tick_base : 0) + a.tick_off;
   const float2* tw = stage_twiddles<N, E>(smem + CS::kTw, a.tw);  // block barrier
   float* mod = reinterpret_cast<float*>(smem + CS::kMod);
@@ -238,6 +257,7 @@ __global__ void __launch_bounds__(kColSbThreads, 2) col_pass_sb_kernel(PassArgs 
   load_slot(&sl[0], &a.slots[i0.slot]);
   if (i1.slot >= 0) load_slot(&sl[1], &a.slots[i1.slot]);
   __syncthreads();
+  pdl_wait_prev();  // the planes (and the transposed modulus) are earlier kernels' output
   copy_col_mod<N, E, TH>(sl[0], i0.block, tick, mod);
   asm volatile("cp.async.commit_group;" ::: "memory");
   if (col_projects(sl[0], tick)) copy_col_tile<N, E, TH>(sl[0].g, i0.block, tile);
@@ -280,16 +300,32 @@ constexpr size_t col_smem_bytes() {
 template <int N, int E>
 constexpr size_t row_smem_bytes() { return (size_t)RowSmem<N, E>::kTotal * sizeof(float2); }
 
+// Launch with programmatic stream serialization (see pdl_allow_next).
+template <class K>
+cudaError_t launch_pdl(K kernel, int grid, int threads, size_t smem, cudaStream_t st,
+                       const PassArgs& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int N, int E>
 cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& a) {
   if (which == 0) {
     if constexpr (col_single_buffered(N, E))
-      col_pass_sb_kernel<N, E><<<grid, kColSbThreads, col_smem_bytes<N, E>(), st>>>(a);
+      return launch_pdl(col_pass_sb_kernel<N, E>, grid, kColSbThreads, col_smem_bytes<N, E>(), st, a);
     else
-      col_pass_kernel<N, E><<<grid, kThreads, col_smem_bytes<N, E>(), st>>>(a);
-  } else
-    row_pass_kernel<N, E><<<grid, kThreads, row_smem_bytes<N, E>(), st>>>(a);
-  return cudaGetLastError();
+      return launch_pdl(col_pass_kernel<N, E>, grid, kThreads, col_smem_bytes<N, E>(), st, a);
+  }
+  return launch_pdl(row_pass_kernel<N, E>, grid, kThreads, row_smem_bytes<N, E>(), st, a);
 }
 
 // occupancy[0] = resident column-pass CTAs per SM, occupancy[1] = row-pass
