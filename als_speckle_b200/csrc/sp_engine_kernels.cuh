@@ -144,6 +144,36 @@ __device__ __forceinline__ float ld_ro(const float* p) {
   return v;
 }
 
+// Programmatic dependent launch: an engine kernel lets the next kernel of its
+// stream be scheduled as soon as all of its own CTAs run, and that kernel
+// builds its twiddle tables and reads its descriptors (nothing an earlier
+// kernel writes) while this one finishes, then waits for it to complete
+// before touching any plane.  The wait is the hardware's grid dependency: it
+// ends when the earlier grid has completed and its writes are visible.
+__device__ __forceinline__ void pdl_allow_next() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait_prev() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launch with programmatic stream serialization (see pdl_allow_next).
+template <class Args>
+cudaError_t launch_pdl(void (*kernel)(Args), int grid, int threads, size_t smem, cudaStream_t st,
+                       const Args& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 // Asynchronous global -> shared copies (cp.async, no registers held): psi,
 // support and modulus tiles are requested at the start of an item and land
 // while the item's first FFT runs.

@@ -16,18 +16,6 @@ struct PassArgs {
   int reverse;  // walk the item list from its end
 };
 
-// Programmatic dependent launch: a pass kernel lets the next kernel of its
-// stream be scheduled as soon as all of its own CTAs run, and that kernel
-// builds its twiddle tables and reads its descriptors (nothing an earlier
-// kernel writes) while this one finishes, then waits for it to complete
-// before touching any plane.  The wait is the hardware's grid dependency: it
-// ends when the earlier grid has completed and its writes are visible.
-__device__ __forceinline__ void pdl_allow_next() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-__device__ __forceinline__ void pdl_wait_prev() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-}
 
 
 // Copy one slot descriptor into shared memory (word by word).
@@ -299,23 +287,6 @@ constexpr size_t col_smem_bytes() {
 }
 template <int N, int E>
 constexpr size_t row_smem_bytes() { return (size_t)RowSmem<N, E>::kTotal * sizeof(float2); }
-
-// Launch with programmatic stream serialization (see pdl_allow_next).
-template <class K>
-cudaError_t launch_pdl(K kernel, int grid, int threads, size_t smem, cudaStream_t st,
-                       const PassArgs& a) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(threads);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, a);
-}
 
 template <int N, int E>
 cudaError_t launch_pass_t(int which, int grid, cudaStream_t st, const PassArgs& a) {
