@@ -109,7 +109,13 @@ int sp_device_init(void);
  * Bytes of workspace that sp_engine_run needs for these trials. */
 int sp_engine_workspace_size(const sp_trial* trials, int n_trials, size_t* bytes);
 /* Run every trial's iterations (uneven sizes and algorithms allowed), write
- * the final psi_in, the crop into save_dev and the per-iteration errors. */
+ * the final psi_in, the crop into save_dev and the per-iteration errors.
+ * The pass kernels are launched with programmatic stream serialization and
+ * let the next kernel of the stream start early: work the caller enqueues
+ * afterwards with plain launches, copies or events sees the results as usual;
+ * a caller kernel launched itself with programmatic stream serialization must
+ * wait for its predecessor grid (cudaGridDependencySynchronize) before
+ * reading them. */
 int sp_engine_run(const sp_trial* trials, int n_trials, void* workspace_dev,
                   size_t workspace_bytes, const sp_run_opts* opts, sp_stream_t stream);
 /* Destroy the CUDA graphs cached by sp_engine_run (call before freeing a
