@@ -525,6 +525,7 @@ def run_ours(args):
     achieved = BYTES_PER_PX * N * N * group / per_tick / 1e9
     plain = run_plain(torch, device, M, S)
     single = run_single_trial(torch, device, M, S, engine)
+    cufft = run_cufft_pair(torch, device, per_tick, group)
     serving = run_serving() if world == 1 and args.serving else None
 
     if world > 1:
@@ -561,6 +562,7 @@ def run_ours(args):
         "fft_tflops": 10.0 * N * N * math.log2(N * N) * group / per_tick / 1e12,
         "plain_gpu": plain,
         "single_trial_engine": single,
+        "cufft_transforms_only": cufft,
         "batched_over_plain": value / world / plain["value"],
         "batched_over_single_trial_engine": value / world / single["value"],
         "clocks": clk.summary(),
@@ -649,6 +651,27 @@ def run_plain(torch, device, M, S, iters=40):
     dt = time.perf_counter() - t0
     return {"value": iters / dt, "unit": "iter/s", "what": "1 trial, cuFFT + elementwise kernels, "
             "sync after every launch (reference GPU dataflow)"}
+
+
+def run_cufft_pair(torch, device, per_tick, group, reps=20):
+    """cuFFT (through torch.fft) on the same planes: a forward and an inverse
+    2-D transform of ``group`` 512^2 complex64 planes, beside one engine tick
+    (the whole iteration: both transforms, the projection and the update)."""
+    x = torch.randn(group, N, N, dtype=torch.complex64, device=device)
+    for _ in range(3):
+        y = torch.fft.ifft2(torch.fft.fft2(x))
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        y = torch.fft.ifft2(torch.fft.fft2(x))
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    del x, y
+    return {"fft2_ifft2_ms": ms, "engine_tick_ms": 1e3 * per_tick,
+            "what": "torch.fft.fft2 then ifft2 of %d planes of %d^2 (cuFFT), against one engine "
+                    "iteration tick of the same trials" % (group, N)}
 
 
 def run_single_trial(torch, device, M, S, engine, iters=200):
